@@ -1,0 +1,234 @@
+"""Generates the golden fixtures in this folder by running the reference here.
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+The reference (a Python package) is imported from its source tree with a stub
+``matplotlib`` (only ``use`` and an empty ``pyplot`` are needed on the compute
+path).  Every fixture stores the reference's inputs and outputs, so tests check
+the oracle and the CUDA path without the reference present.
+
+Fixtures:
+  trace_*.npz   tracer inputs (particles, fields, barrier) and trace_cpu outputs
+                (trench_charging_2d.py:542-702), with per-particle record data
+  run_*.npz     short run() batch loops: rho_raw, mean_phi, history
+                (trench_charging_2d.py:1045-1369)
+  fields_*.npz  setup_fields / solve / compute_field / build_leakage /
+                conductor_response outputs for one geometry
+  regression_pin.json  agreement of run() here with the reference's own
+                tests/data/*.npz (tests/test_regression.py:41-50)
+"""
+import json
+import sys
+import tempfile
+import types
+from dataclasses import asdict, replace
+from pathlib import Path
+
+import numpy as np
+
+OUT = Path(__file__).resolve().parent
+
+
+def import_reference(path):
+    stub = Path(tempfile.mkdtemp()) / "matplotlib"
+    stub.mkdir()
+    (stub / "__init__.py").write_text("def use(*a, **k):\n    pass\n")
+    (stub / "pyplot.py").write_text("")
+    sys.path.insert(0, str(stub.parent))
+    sys.path.insert(0, str(path))
+    import trench_charging_2d as T
+    import trench_rf as RF
+    return T, RF
+
+
+def params_json(p):
+    return json.dumps(asdict(p))
+
+
+def save(name, **arrays):
+    np.savez_compressed(OUT / name, **arrays)
+    size = (OUT / name).stat().st_size
+    print(f"wrote {name} ({size/1024:.0f} KiB)")
+
+
+def trace_case(T, name, p, phi, fields, solid, seed, n, barrier=True, rf=None, ion_energy=None, rng=None):
+    ex, ey = T.compute_field(phi, ~solid, p, fields["volts"]["top"])
+    wface = np.where(fields["cond"], 1.0, fields["eps"] / (1 + fields["eps"]))
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    parts = T.inject(p, n, solid.shape[1], rng, ion_energy)
+    bar = (phi, wface) if barrier else None
+    out = {}
+    for rec in (False, True):
+        record = {} if rec else None
+        res = T.trace_cpu(*(v.copy() for v in parts), ex, ey, ~solid, p, bar, record, rf=rf)
+        if not rec:
+            out.update(cnt_i=res[0], cnt_e=res[1], escaped=res[2], lost=np.int64(res[3]))
+        else:
+            out.update(rec_cnt_i=res[0], rec_cnt_e=res[1], rec_escaped=res[2], rec_lost=np.int64(res[3]),
+                       rec_status=record["status"], rec_hit_cells=record["hit_cells"],
+                       rec_endpoints=record["endpoints"], rec_final_velocity=record["final_velocity"],
+                       rec_selected=record["selected"],
+                       rec_path_lengths=np.array([len(v) for v in record["paths"]]),
+                       rec_paths=np.concatenate(record["paths"]) if record["paths"] else np.zeros((0, 2)))
+            if rf is not None:
+                out.update(rec_flight_time=record["flight_time"], rec_final_phase=record["final_phase"])
+    extra = {}
+    if rf is not None:
+        extra = dict(rf_period=rf["period"], rf_dt_max=rf["dt_max"], rf_wave=rf["wave"], rf_phi=rf["phi"],
+                     rf_Ex=rf["Ex"], rf_Ey=rf["Ey"], rf_initial_time=rf["initial_time"])
+    x, y, vx, vy, qm, spc = parts
+    save(f"trace_{name}.npz", params=params_json(p), solid=solid, x=x, y=y, vx=vx, vy=vy, qm=qm, spc=spc,
+         Ex=ex, Ey=ey, phi=phi, wface=wface, barrier=np.bool_(barrier), **out, **extra)
+
+
+def charged_state(T, p, n_batches):
+    """Reference run() for a few batches; returns its charged potential."""
+    res = T.run(replace(p, n_batches=n_batches), log=lambda s: None)
+    return res["mean_phi"], res
+
+
+def main(ref):
+    T, RF = import_reference(ref)
+    P = T.Params
+
+    # --- tracer cases -------------------------------------------------------
+    small = replace(P(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc", sigma_s=0,
+                    n_batches=8, n_per_batch=400, max_steps=1000, probe_trajectories=12)
+    solid, mask, i0, i1 = T.build_geometry(small)
+    f = T.setup_fields(small, solid, mask)
+    rho = np.zeros(solid.shape)
+    rho[i0 - 1, small.floor_t:small.floor_t + small.trench_d] = 2e7
+    rho[i1, small.floor_t:small.floor_t + small.trench_d] = -1e7
+    phi = f["solve"]((-rho / T.EPS0).ravel()).reshape(solid.shape)
+    for wall in ("barrier", "absorb"):
+        trace_case(T, f"small_{wall}", replace(small, wall_model=wall), phi, f, solid, 20, 400,
+                   barrier=wall == "barrier")
+
+    tr, ma = np.degrees(np.arctan(.25)), np.degrees(np.arctan(.5))
+    taper = replace(P(), nx=40, trench_w=16, trench_d=20, floor_t=4, mask_t=12, n_vac=10, trench_taper_deg=tr,
+                    mask_taper_deg=ma, bias="dc", sigma_s=0, n_per_batch=256, max_steps=800,
+                    field_mode="fixed", substrate_voltage=-30, mask_voltage=-10, probe_trajectories=12)
+    solid, mask, i0, i1 = T.build_geometry(taper)
+    f = T.setup_fields(taper, solid, mask)
+    regions = T.charge_monitors(solid, mask, i0, i1, taper)
+    rho = np.zeros(solid.shape)
+    rho.ravel()[regions["left"]] = 2e6
+    rho.ravel()[regions["right"]] = -1e6
+    phi = f["solve"]((-rho / T.EPS0).ravel()).reshape(solid.shape) + f["external"]
+    for wall in ("barrier", "absorb"):
+        trace_case(T, f"taper_{wall}", replace(taper, wall_model=wall), phi, f, solid, 22, 256,
+                   barrier=wall == "barrier")
+
+    # Configuration-1 geometry (80x200, conductive floating mask), charged by 6 batches.
+    cfg1 = replace(P(), dx=5e-9, nx=80, trench_w=20, trench_d=60, floor_t=20, mask_t=20, n_vac=100,
+                   mask_type="conductor", field_mode="floating", sigma_s=1e-15, wall_model="barrier", bias="dc",
+                   ion_energy_eV=100, electron_temp_eV=4, n_per_batch=2000, seed=0, probe_trajectories=16)
+    phi, _ = charged_state(T, cfg1, 6)
+    solid, mask, _, _ = T.build_geometry(cfg1)
+    f = T.setup_fields(cfg1, solid, mask)
+    trace_case(T, "cfg1", cfg1, phi, f, solid, 100, 2000)
+
+    # Configuration-2 geometry (60x250 AR 8, tapers 2/5 deg, dielectric mask), charged by 6 batches.
+    cfg2 = replace(P(), nx=60, trench_w=20, trench_d=160, floor_t=10, mask_t=20, n_vac=60, trench_taper_deg=2.0,
+                   mask_taper_deg=5.0, mask_type="dielectric", mask_eps_r=3.0, electron_temp_eV=3.0, bias="dc",
+                   ion_energy_eV=90.0, n_per_batch=2000, seed=1, probe_trajectories=16)
+    phi, _ = charged_state(T, cfg2, 6)
+    solid, mask, _, _ = T.build_geometry(cfg2)
+    f = T.setup_fields(cfg2, solid, mask)
+    trace_case(T, "cfg2", cfg2, phi, f, solid, 101, 2000)
+
+    # RF in-flight clock on a tapered trench (test_taper.py:273-294 waveform).
+    rfp = replace(taper, bias="rf", field_mode="circuit_rf", side_bc="pillar", rf_freq=5e8)
+    t = np.arange(256) / 256 / rfp.rf_freq
+    c = dict(t=t, uw=-60 - 20 * np.sin(2 * np.pi * t * rfp.rf_freq), um=-30 - 10 * np.sin(2 * np.pi * t * rfp.rf_freq),
+             up=t * 0, V1=30 + 10 * np.sin(2 * np.pi * t * rfp.rf_freq))
+    solid, mask, _, _ = T.build_geometry(rfp)
+    f = T.setup_fields(rfp, solid, mask, c)
+    rng = np.random.default_rng(3)
+    n = 512
+    parts_rng = np.random.default_rng(3)
+    rf = {**f["rf"], "initial_time": np.concatenate([RF.launch_times(np.random.default_rng(4), n, f["rf"]["period"])
+                                                     for _ in range(2)])}
+    trace_case(T, "rf_taper", rfp, f["external"], f, solid, 3, n, rf=rf,
+               ion_energy=lambda r, k: np.full(k, rfp.electron_temp_eV / 2), rng=parts_rng)
+    del rng
+
+    # --- batch-loop runs ----------------------------------------------------
+    base = dict(nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc", n_per_batch=400,
+                max_steps=1000, n_batches=4)
+    runs = {
+        "floating_leak": replace(P(), sigma_s=1e-14, **base),
+        "floating_noleak": replace(P(), sigma_s=0.0, **base),
+        "fixed_leak": replace(P(), sigma_s=1e-14, field_mode="fixed", substrate_voltage=-20, mask_voltage=-10,
+                              **base),
+        "dielectric_leak": replace(P(), sigma_s=1e-14, mask_type="dielectric", **base),
+        "absorb_leak": replace(P(), sigma_s=1e-14, wall_model="absorb", **base),
+        "taper_leak": replace(P(), nx=40, trench_w=16, trench_d=20, floor_t=4, mask_t=12, n_vac=10,
+                              trench_taper_deg=tr, mask_taper_deg=ma, bias="dc", sigma_s=1e-14, n_per_batch=256,
+                              max_steps=800, n_batches=3),
+    }
+    for name, p in runs.items():
+        res = T.run(p, log=lambda s: None)
+        save(f"run_{name}.npz", params=params_json(p), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
+             solid=res["solid"], mask=res["mask"],
+             **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
+
+    # --- field-side cases -----------------------------------------------------
+    for name, p in {"floating": runs["floating_leak"], "fixed": runs["fixed_leak"],
+                    "dielectric": runs["dielectric_leak"],
+                    "cfg2": replace(cfg2, sigma_s=1e-15)}.items():
+        solid, mask, i0, i1 = T.build_geometry(p)
+        f = T.setup_fields(p, solid, mask)
+        rng = np.random.default_rng(7)
+        rho = np.zeros(solid.shape)
+        surf = T.surface_cells(solid)
+        rho[surf] = rng.normal(0, 3e6, surf.sum())
+        if f["cond"].any():
+            rho[f["cond"]] = 0.0
+            c_cell = np.flatnonzero(surf & f["cond"])[0]
+            rho.flat[c_cell] = 5e6
+        phi = f["solve"]((-rho / T.EPS0).ravel()).reshape(solid.shape) + f["external"]
+        ex, ey = T.compute_field(phi, ~solid, p, f["volts"]["top"])
+        leak = T.build_leakage(solid, f["solve"], i0, i1, p)
+        extra = {}
+        if f["floating"]:
+            g = T.conductor_response(f["solve"], f["cond"], p.dx)
+            extra = dict(g_cond=g, C_cond=1.0 / g[f["cond"]][0])
+        m = len(leak["flat"])
+        if m <= 200:
+            extra["leak_M"] = leak["M"]
+        else:
+            # Large operators are pinned through their action on seeded vectors.
+            extra["leak_MQ"] = leak["M"] @ np.random.default_rng(11).normal(size=(m, 4))
+        save(f"fields_{name}.npz", params=params_json(p), solid=solid, mask=mask, rho=rho, phi=phi, Ex=ex, Ey=ey,
+             external=f["external"], leak_flat=leak["flat"], leak_region=leak["region"], **extra)
+
+    # conductor_step values (trench_charging_2d.py:815-830)
+    cases = [(120, 80, 3e-12, 2e-10, 3.0, 0.0), (0, 50, 1e-12, 1e-10, 4.0, 0.01), (40, 0, 1e-12, 1e-10, 4.0, -0.2),
+             (500, 500, 2e-12, 3e-10, 3.0, 0.05), (10, 900, 1e-12, 1e-10, 2.0, 0.0)]
+    vals = [T.conductor_step(*c) for c in cases]
+    save("conductor_step.npz", args=np.array(cases, dtype=float), values=np.array(vals))
+
+    # --- agreement with the reference's own regression data -------------------
+    pin = {}
+    data = Path(ref) / "tests" / "data"
+    for name, sigma in (("base_noleak", 0.0), ("base_leak", 1e-14)):
+        p = replace(P(), mask_t=0, n_batches=40, bias="dc", sigma_s=sigma, wall_model="absorb")
+        res = T.run(p, log=lambda s: None)
+        with np.load(data / f"{name}.npz") as d:
+            pin[name] = dict(
+                rho_max_abs_diff=float(np.max(np.abs(d["rho"] - res["rho"]))),
+                phi_max_abs_diff=float(np.max(np.abs(d["phi"] - res["phi"]))),
+                hist_ratio_i_equal=bool(np.array_equal(d["hist_ratio_i_bottom"], res["hist"]["ratio_i_bottom"])),
+                hist_ratio_e_equal=bool(np.array_equal(d["hist_ratio_e_bottom"], res["hist"]["ratio_e_bottom"])))
+            save(f"run_{name}.npz", params=params_json(p), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
+                 solid=res["solid"], mask=res["mask"], ref_data_rho=d["rho"], ref_data_phi=d["phi"],
+                 ref_data_hist_ratio_i_bottom=d["hist_ratio_i_bottom"],
+                 ref_data_hist_ratio_e_bottom=d["hist_ratio_e_bottom"],
+                 **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
+    (OUT / "regression_pin.json").write_text(json.dumps(pin, indent=1) + "\n")
+    print(json.dumps(pin, indent=1))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

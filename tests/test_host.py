@@ -1,0 +1,77 @@
+"""Host-side setup mirrors the reference: geometry, injection, validation. CPU only."""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from trench_b200 import geometry, inject
+from trench_b200.params import Params
+
+
+def small(**kw):
+    base = dict(nx=20, trench_w=6, trench_d=12, floor_t=4, mask_t=4, n_vac=8, bias="dc")
+    return replace(Params(), **{**base, **kw})
+
+
+@pytest.mark.parametrize("name", ["trace_small_barrier", "trace_taper_barrier", "trace_cfg1", "trace_cfg2",
+                                  "fields_dielectric"])
+def test_geometry_matches_reference(name):
+    g = load_golden(f"{name}.npz")
+    solid, mask, _, _ = geometry.build_geometry(g["p"])
+    np.testing.assert_array_equal(solid, g["solid"])
+    if "mask" in g:
+        np.testing.assert_array_equal(mask, g["mask"])
+
+
+@pytest.mark.parametrize("name", ["trace_small_barrier", "trace_cfg1", "trace_cfg2"])
+def test_injection_reproduces_reference_particles(name):
+    g = load_golden(f"{name}.npz")
+    p = g["p"]
+    seed = {"trace_small_barrier": 20, "trace_cfg1": 100, "trace_cfg2": 101}[name]
+    n = len(g["x"]) // 2
+    parts = inject.inject(p, n, g["solid"].shape[1], np.random.default_rng(seed))
+    for k, v in zip(("x", "y", "vx", "vy", "qm", "spc"), parts):
+        np.testing.assert_array_equal(v, g[k])
+
+
+@pytest.mark.parametrize("offset", [-6, 0, 6])
+def test_shifted_opening(offset):
+    """trench tests/test_features.py:23-30"""
+    p = small(trench_offset=offset)
+    solid, mask, i0, i1 = geometry.build_geometry(p)
+    assert i0 == 7 + offset and i1 == 13 + offset
+    assert not solid[i0:i1, p.floor_t:].any()
+    assert np.array_equal(mask, solid & (np.arange(solid.shape[1])[None, :] >= 16))
+
+
+@pytest.mark.parametrize("changes", [dict(trench_offset=-7), dict(trench_offset=7), dict(trench_offset=0.5),
+                                     dict(trench_taper_deg=90), dict(mask_taper_deg=np.nan),
+                                     dict(trench_taper_deg=40), dict(mask_type="metal"), dict(mask_t=-1)])
+def test_invalid_geometry_is_rejected(changes):
+    with pytest.raises(ValueError):
+        geometry.build_geometry(small(**changes))
+
+
+def test_tapered_openings_match_reference_known_answers():
+    """trench tests/test_taper.py:53-69"""
+    tr, ma = np.degrees(np.arctan(.25)), np.degrees(np.arctan(.5))
+    p = replace(Params(), nx=40, trench_w=16, trench_d=20, floor_t=4, mask_t=12, n_vac=10,
+                trench_taper_deg=tr, mask_taper_deg=ma)
+    solid, mask, i0, i1 = geometry.build_geometry(p)
+    assert (i0, i1) == (12, 28)
+    assert geometry.opening_span(solid, p.floor_t) == (17, 23)
+    assert geometry.opening_span(solid, p.floor_t + p.trench_d - 1) == (12, 28)
+    assert geometry.opening_span(solid, p.floor_t + p.trench_d + p.mask_t - 1) == (6, 34)
+    np.testing.assert_array_equal(solid, solid[::-1])
+
+
+def test_samplers_shapes_and_ranges():
+    p = Params()
+    rng = np.random.default_rng(0)
+    e = inject.mixture_energy([(0.5, "normal", 40, 6), (0.5, "normal", 140, 6)])(rng, 10000)
+    assert abs(np.mean(e) - 90) < 1.5
+    vx, vy = inject.energy_angle_sampler(p, lambda r, n: np.full(n, 100.0), inject.half_gaussian_angle(3))(rng, 5000)
+    assert (vy < 0).all()
+    ang = np.degrees(np.arctan2(vx, -vy))
+    assert 2.0 < np.std(ang) < 4.0 and abs(np.mean(ang)) < 0.2

@@ -1,0 +1,247 @@
+"""CUDA tracer parity: B200Tracer (through the C ABI) against the reference outputs
+(golden fixtures) and the oracle.  Mirrors the reference's own CPU/CUDA tests
+(tests/test_cuda.py:49-146, tests/test_taper.py:197-270, tests/test_features.py:135-163).
+"""
+import threading
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import oracle_trace as OT
+from trench_b200 import geometry, inject
+from trench_b200.params import Params
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["small_barrier", "small_absorb", "taper_barrier", "taper_absorb", "cfg1", "cfg2"]
+
+
+def rf_of(g):
+    if "rf_period" not in g:
+        return None
+    return dict(period=float(g["rf_period"]), dt_max=float(g["rf_dt_max"]), wave=g["rf_wave"], phi=g["rf_phi"],
+                Ex=g["rf_Ex"], Ey=g["rf_Ey"], initial_time=g["rf_initial_time"])
+
+
+def parts(g):
+    return [g[k].copy() for k in ("x", "y", "vx", "vy", "qm", "spc")]
+
+
+def barrier(g):
+    return (g["phi"], g["wface"]) if bool(g["barrier"]) else None
+
+
+@pytest.fixture(scope="module")
+def tracers(cuda_device):
+    from trench_b200.tracer import B200Tracer
+    cache = {}
+
+    def get(solid, precision):
+        key = (solid.shape, solid.tobytes(), precision)
+        if key not in cache:
+            cache[key] = B200Tracer(~solid, cuda_device, precision=precision)
+        return cache[key]
+    return get
+
+
+@pytest.mark.parametrize("name", CASES + ["rf_taper"])
+def test_f64_counts_equal_reference(tracers, name):
+    g = load_golden(f"trace_{name}.npz")
+    t = tracers(g["solid"], "f64")
+    got = t(*parts(g), np.asfortranarray(g["Ex"]), np.asfortranarray(g["Ey"]), ~g["solid"], g["p"], barrier(g),
+            rf=rf_of(g))
+    np.testing.assert_array_equal(got[0], g["cnt_i"])
+    np.testing.assert_array_equal(got[1], g["cnt_e"])
+    np.testing.assert_array_equal(got[2], g["escaped"])
+    assert got[3] == int(g["lost"])
+
+
+@pytest.mark.parametrize("name", CASES + ["rf_taper"])
+def test_f64_record_matches_reference(tracers, name):
+    g = load_golden(f"trace_{name}.npz")
+    t = tracers(g["solid"], "f64")
+    rec = {}
+    got = t(*parts(g), g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g), record=rec, rf=rf_of(g))
+    np.testing.assert_array_equal(got[0], g["rec_cnt_i"])
+    np.testing.assert_array_equal(got[1], g["rec_cnt_e"])
+    for k in ("selected", "status", "hit_cells"):
+        np.testing.assert_array_equal(rec[k], g[f"rec_{k}"])
+    np.testing.assert_allclose(rec["endpoints"], g["rec_endpoints"], rtol=1e-10, atol=1e-13)
+    np.testing.assert_allclose(rec["final_velocity"], g["rec_final_velocity"], rtol=1e-10, atol=1e-13)
+    np.testing.assert_array_equal([len(v) for v in rec["paths"]], g["rec_path_lengths"])
+    if len(rec["paths"]):
+        np.testing.assert_allclose(np.concatenate(rec["paths"]), g["rec_paths"], rtol=1e-10, atol=1e-15)
+    if rf_of(g) is not None:
+        np.testing.assert_allclose(rec["flight_time"], g["rec_flight_time"], rtol=1e-10, atol=1e-22)
+        np.testing.assert_allclose(rec["final_phase"], g["rec_final_phase"], rtol=1e-10, atol=1e-8)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_f64_per_particle_equals_oracle(tracers, name):
+    """Per-particle status, absorbing cell and step count are identical to the oracle."""
+    g = load_golden(f"trace_{name}.npz")
+    t = tracers(g["solid"], "f64")
+    t(*parts(g), g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
+    want = OT.trace_detail(*parts(g)[:5], g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
+    np.testing.assert_array_equal(t.last["status"], want["status"])
+    np.testing.assert_array_equal(t.last["hit"], want["hit"])
+    np.testing.assert_array_equal(t.last["steps"], want["steps"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_f32_hits_agree_with_fp64_oracle(tracers, name):
+    """FP32 mode: per-particle absorbing cells agree with the FP64 oracle; per-cell
+    counts are bit-exact wherever the hits agree (they are integer atomics)."""
+    g = load_golden(f"trace_{name}.npz")
+    t = tracers(g["solid"], "f32")
+    got = t(*parts(g), g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
+    want = OT.trace_detail(*parts(g)[:5], g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
+    same = (t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])
+    n = len(same)
+    assert same.mean() >= 0.99, f"agreement {same.mean():.5f}"
+    # counts restricted to agreeing particles are identical by construction; the
+    # totals differ by at most the disagreeing particles
+    total = got[0].sum() + got[1].sum() + got[2].sum() + got[3]
+    assert total == n
+    diff = np.abs(got[0] - OT.counts_from_detail(want, g["spc"], g["solid"].shape)[0]).sum()
+    assert diff <= 2 * (~same).sum()
+
+
+def test_f32_large_sample_agreement_and_bottom_flux(tracers):
+    """2^16 particles/species on the charged AR-8 geometry: hit-cell agreement with
+    the FP64 oracle >= 99.9% and bottom ion/electron flux within 3 sigma."""
+    g = load_golden("trace_cfg2.npz")
+    p = g["p"]
+    solid = g["solid"]
+    n = 1 << 16
+    x, y, vx, vy, qm, spc = inject.inject(p, n, solid.shape[1], np.random.default_rng(123))
+    t = tracers(solid, "f32")
+    got = t(x, y, vx, vy, qm, spc, g["Ex"], g["Ey"], ~solid, p, barrier(g))
+    want = OT.trace_detail(x, y, vx, vy, qm, g["Ex"], g["Ey"], ~solid, p, barrier(g))
+    same = (t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])
+    agree = same.mean()
+    ref = OT.counts_from_detail(want, spc, solid.shape)
+    b0, b1 = geometry.opening_span(solid, p.floor_t)
+    for k in (0, 1):
+        a = got[k][b0:b1, p.floor_t - 1].sum()
+        r = ref[k][b0:b1, p.floor_t - 1].sum()
+        sigma = np.sqrt(max(r, 1))
+        assert abs(a - r) <= 3 * sigma, (k, a, r)
+    assert agree >= 0.999, f"hit agreement {agree:.5f}"
+
+
+def test_empty_launch(tracers):
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12)
+    solid, _, _, _ = geometry.build_geometry(p)
+    z = np.zeros(solid.shape)
+    e = np.zeros(0)
+    rec = {}
+    ci, ce, esc, lost = tracers(solid, "f64")(e, e, e, e, e, np.zeros(0, np.int8), z, z, ~solid, p, record=rec)
+    assert ci.sum() == ce.sum() == esc.sum() == lost == 0
+    assert rec["paths"] == []
+
+
+def test_cancellation_keeps_initial_paths(tracers):
+    """trench tests/test_cuda.py:82-92"""
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, probe_trajectories=12)
+    solid, _, _, _ = geometry.build_geometry(p)
+    prt = inject.inject(p, 20, solid.shape[1], np.random.default_rng(1))
+    stop = threading.Event()
+    stop.set()
+    rec = {}
+    z = np.zeros(solid.shape)
+    ci, ce, esc, lost = tracers(solid, "f64")(*prt, z, z, ~solid, p, record=rec, stop=stop)
+    assert ci.sum() == ce.sum() == esc.sum() == 0 and lost == 40
+    assert rec["cancelled"] and all(v.shape == (1, 2) for v in rec["paths"])
+    np.testing.assert_array_equal(rec["endpoints"], np.column_stack(prt[:2]))
+
+
+def test_chunked_run_with_stop_equals_single_launch(tracers):
+    g = load_golden("trace_cfg1.npz")
+    t = tracers(g["solid"], "f64")
+    a = t(*parts(g), g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
+    b = t(*parts(g), g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g), stop=threading.Event())
+    for u, v in zip(a, b):
+        np.testing.assert_array_equal(u, v)
+
+
+def test_invalid_device_is_reported(cuda_device):
+    from trench_b200.tracer import B200Tracer
+    with pytest.raises(RuntimeError, match="デバイス"):
+        B200Tracer(np.ones((4, 5), bool), device=999)
+
+
+def test_input_validation(tracers):
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12)
+    solid, _, _, _ = geometry.build_geometry(p)
+    t = tracers(solid, "f32")
+    z = np.zeros(solid.shape)
+    one = np.ones(1)
+    with pytest.raises(ValueError):
+        t(one, one, one, one, one, np.array([2], np.int8), z, z, ~solid, p)
+    with pytest.raises(ValueError):
+        t(one, one, one, one, one, np.zeros(1, np.int8), z[:-1], z, ~solid, p)
+    with pytest.raises(ValueError):
+        t(one, one, one, one, one, np.zeros(1, np.int8), z, z, ~solid, replace(p, cfl=1.5))
+    with pytest.raises(ValueError):
+        t(one, one, one, one, one, np.zeros(1, np.int8), z, z, solid, p)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("reflect,recording", [(False, False), (False, True), (True, True), (True, False)])
+def test_first_wall_face_when_both_end_cells_are_vacuum(tracers, precision, reflect, recording):
+    """trench tests/test_taper.py:197-226 (staircase corner contact)."""
+    if recording and precision == "f32":
+        pytest.skip("record runs on the FP64 kernel")
+    tr, ma = np.degrees(np.arctan(.25)), np.degrees(np.arctan(.5))
+    p = replace(Params(), nx=40, trench_w=16, trench_d=20, floor_t=4, mask_t=12, n_vac=10, trench_taper_deg=tr,
+                mask_taper_deg=ma, max_steps=1, probe_trajectories=12)
+    solid, _, _, _ = geometry.build_geometry(p)
+    vac = ~solid
+    corners = solid[:, :-1] & vac[:, 1:] & np.roll(vac, -1, axis=0)[:, :-1]
+    cx, cy = np.argwhere(corners)[0]
+    x, y = np.array([(cx + .92) * p.dx]), np.array([(cy + 1.02) * p.dx])
+    phi = np.zeros(solid.shape)
+    phi[cx, cy] = 1e6
+    bar = (phi, np.ones_like(phi)) if reflect else None
+    rec = {} if recording else None
+    t = tracers(solid, precision)
+    ci, _, _, lost = t(x, y, np.array([1000.]), np.array([-1000.]), np.ones(1), np.zeros(1, dtype=np.int8),
+                       np.zeros_like(phi), np.zeros_like(phi), vac, p, bar, record=rec)
+    if reflect:
+        assert lost == 1 and ci.sum() == 0
+        if recording:
+            np.testing.assert_array_equal(rec["final_velocity"], [[1000., 1000.]])
+            np.testing.assert_allclose(rec["endpoints"], [[(cx + .92) * p.dx, (cy + 1.02) * p.dx]], atol=1e-20)
+    else:
+        assert lost == 0 and ci[cx, cy] == 1
+        if recording:
+            assert rec["hit_cells"].tolist() == [[cx, cy]]
+            assert rec["endpoints"][0, 1] == pytest.approx((cy + 1) * p.dx, abs=1e-20)
+
+
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+@pytest.mark.parametrize("trench_angle,mask_angle,mask_t,fraction", [
+    (np.degrees(np.arctan(.25)), np.degrees(np.arctan(.5)), 12, 6 / 28),
+    (-np.degrees(np.arctan(.25)), np.degrees(np.arctan(.5)), 12, 16 / 28),
+    (np.degrees(np.arctan(.25)), -np.degrees(np.arctan(.5)), 12, 1),
+    (np.degrees(np.arctan(.25)), 0, 0, 6 / 16)])
+def test_vertical_beam_matches_ballistic_aperture(tracers, precision, trench_angle, mask_angle, mask_t, fraction):
+    """trench tests/test_taper.py:132-157: exactly vertical ions over the entrance."""
+    p = replace(Params(), nx=40, trench_w=16, trench_d=20, floor_t=4, mask_t=mask_t, n_vac=10,
+                trench_taper_deg=trench_angle, mask_taper_deg=mask_angle, max_steps=800)
+    solid, _, _, _ = geometry.build_geometry(p)
+    ny = solid.shape[1]
+    i0, i1 = geometry.opening_span(solid, p.floor_t + p.trench_d + p.mask_t - 1)
+    b0, b1 = geometry.opening_span(solid, p.floor_t)
+    n = (i1 - i0) * 8
+    x = (i0 + (np.arange(n) + 0.5) * (i1 - i0) / n) * p.dx
+    y = np.full(n, (ny - 1e-3) * p.dx)
+    v = np.sqrt(2 * 100 * 1.602176634e-19 / (40 * 1.66053906660e-27))
+    z = np.zeros(solid.shape)
+    ci, _, esc, lost = tracers(solid, precision)(x, y, np.zeros(n), np.full(n, -v), np.full(n, 2.4e6),
+                                                 np.zeros(n, np.int8), z, z, ~solid, p)
+    assert ci[b0:b1, p.floor_t - 1].sum() / n == fraction
+    assert esc.sum() == lost == 0 and ci.sum() == n

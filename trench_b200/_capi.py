@@ -1,0 +1,95 @@
+"""ctypes binding of libtrench_b200.so (the C ABI in include/trench_b200.h).
+
+The library is built in-tree by ``trench_b200.build``.  Loading fails loudly: there
+is no CPU fallback anywhere in this package.
+"""
+import ctypes
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libtrench_b200.so"
+
+TB_OK = 0
+TB_ERR_ARG = 1
+TB_ERR_CUDA = 2
+TB_ERR_DEVICE = 3
+TB_ERR_KERNEL = 4
+TB_ERR_CONVERGENCE = 5
+PRECISION = {"f64": 0, "f32": 1}
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+_i64 = ctypes.c_int64
+_dbl = ctypes.c_double
+
+
+class TraceArgs(ctypes.Structure):
+    """Mirror of ``tb_trace_args``; field order and types follow the header."""
+    _fields_ = [
+        ("n", _i64),
+        ("d_x", _vp), ("d_y", _vp), ("d_vx", _vp), ("d_vy", _vp),
+        ("d_qm", _vp), ("d_spc", _vp),
+        ("d_ex", _vp), ("d_ey", _vp),
+        ("d_phi", _vp), ("d_wface", _vp),
+        ("max_steps", ctypes.c_int), ("step_budget", ctypes.c_int),
+        ("cfl", _dbl),
+        ("tapered", ctypes.c_int),
+        ("d_rf_ex", _vp), ("d_rf_ey", _vp), ("d_rf_phi", _vp),
+        ("d_wave", _vp),
+        ("n_phase", ctypes.c_int),
+        ("period", _dbl), ("dt_max", _dbl), ("bound_vs", _dbl), ("bound_vm", _dbl),
+        ("d_clock", _vp),
+        ("record", ctypes.c_int),
+        ("d_endpoints", _vp), ("d_slots", _vp), ("d_paths", _vp), ("d_path_len", _vp),
+        ("path_stride", ctypes.c_int),
+        ("d_counts", _vp), ("d_totals", _vp),
+        ("d_status", _vp), ("d_hit", _vp), ("d_steps", _vp),
+        ("write_state", ctypes.c_int),
+    ]
+
+
+# Every symbol the header declares, with its ctypes signature.
+SIGNATURES = {
+    "tb_version": (ctypes.c_int, []),
+    "tb_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int, _dbl, _vp]),
+    "tb_destroy": (ctypes.c_int, [_vp]),
+    "tb_last_error": (ctypes.c_char_p, [_vp]),
+    "tb_device_info": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    "tb_set_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _vp]),
+    "tb_trace": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs), ctypes.c_int, _vp]),
+    "tb_check": (ctypes.c_int, [_vp, _vp]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the library once; raises RuntimeError if it is missing or incomplete."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH.name} is not built: run trench_b200.build.build() "
+                               "(no CPU fallback exists)")
+        h = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib
+
+
+class TBError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+def raise_for(code, ctx=None):
+    """Map a TB status to the exception the reference raises for the same case."""
+    if code == TB_OK:
+        return
+    msg = lib().tb_last_error(ctx).decode(errors="replace")
+    if code == TB_ERR_ARG:
+        raise ValueError(msg)
+    raise TBError(code, msg)

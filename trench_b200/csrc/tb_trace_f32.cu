@@ -1,0 +1,363 @@
+// FP32 tracer (precision TB_PRECISION_F32): the throughput path.
+//
+// Design (B200-first):
+//  * Position = integer cell + FP32 offset in [0,1) cell units, so the cell
+//    index, periodic wrap and floor are exact integer operations and the offset
+//    keeps 2^-24-cell resolution everywhere in the grid.
+//  * Velocities in units of vscale (m/s); time in dx/vscale; the packed field is
+//    E*vac*dx/vscale^2 so qm*field is the acceleration in these units.
+//  * The packed field (8 bytes per cell, vacuum flag in bit 0 of Ex) is staged
+//    once per block into shared memory with a bulk async copy (TMA engine,
+//    cp.async.bulk + mbarrier); every bilinear gather is a shared-memory load.
+//    Grids too large for shared memory read the same layout from global memory
+//    (L2-resident).
+//  * Persistent warps, one particle per lane, lanes refill from a global atomic
+//    queue as soon as their particle ends (no lane waits for a slow electron).
+//  * Absorbed particles are deposited with integer atomics (bit-exact counts).
+// The step follows the reference algorithm (trench_charging_2d.py:584-650,
+// trench_trace.cu:92-148): vacuum-weighted bilinear field, CFL step, trapezoid
+// update, periodic x, escape at the top, staircase corner crossing, first-face
+// wall entry and the potential-barrier reflection.
+#include "tb_internal.cuh"
+
+namespace {
+
+constexpr int F32_THREADS = 1024;
+constexpr float ONE_BELOW = 0x1.fffffep-1f;  // largest float < 1
+
+struct K32 {
+    tb_trace_args a;
+    int nx, ny;
+    double dx, vscale;
+    float inv_v;                    // the reference's "+1 m/s" in velocity units
+    const tb_fcell *field;          // packed field (global)
+    const float4 *barrier;          // per-cell face barrier, potential / vscale^2
+    unsigned long long *queue;
+    int *err;
+    int bytes;                      // packed field bytes (multiple of 16)
+};
+
+__device__ __forceinline__ float vac_of(const tb_fcell &c) {
+    return (float)(__float_as_uint(c.ex) & 1u);
+}
+
+template <bool SMEM>
+struct FieldView {
+    const tb_fcell *p;
+    __device__ __forceinline__ tb_fcell at(int c) const {
+        if (SMEM) return p[c];
+        const float2 v = __ldg(reinterpret_cast<const float2 *>(p) + c);
+        return tb_fcell{v.x, v.y};
+    }
+    __device__ __forceinline__ bool vac(int c) const {
+        float x;
+        if (SMEM) x = p[c].ex; else x = __ldg(&p[c].ex);
+        return __float_as_uint(x) & 1u;
+    }
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Bulk-copies `bytes` (multiple of 16) from global to shared memory through the
+// async copy engine and waits on an mbarrier with a bounded number of polls.
+// Returns false if the copy did not complete within the bound.
+__device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mbar) {
+    const uint32_t bar = smem_u32(mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        const int chunk = 32768;
+        for (int off = 0; off < bytes; off += chunk) {
+            const int sz = bytes - off < chunk ? bytes - off : chunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                ::"r"(smem_u32((char *)dst + off)), "l"((const char *)src + off), "r"(sz), "r"(bar)
+                : "memory");
+        }
+    }
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done) : "r"(bar) : "memory");
+        if (!done) __nanosleep(32);
+    }
+    return __syncthreads_and(done) != 0;
+}
+
+template <bool SMEM>
+__global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const tb_trace_args &a = k.a;
+    const int nx = k.nx, ny = k.ny;
+    const int cells = nx * ny;
+
+    FieldView<SMEM> F;
+    if (SMEM) {
+        if (!stage_field(smem_raw, k.field, k.bytes, &mbar)) {
+            if (threadIdx.x == 0) atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BULK_TIMEOUT);
+            return;
+        }
+        F.p = reinterpret_cast<const tb_fcell *>(smem_raw);
+    } else {
+        F.p = k.field;
+    }
+
+    const float cfl = (float)a.cfl;
+    const bool barrier = a.d_phi != nullptr;
+    const bool tapered = a.tapered != 0;
+    const bool first_face = barrier || tapered;
+
+    long long pid = -1;
+    int ix = 0, iy = 0, steps = 0, stop_at = 0, spc = 0;
+    float ox = 0.f, oy = 0.f, vx = 0.f, vy = 0.f, qm = 0.f;
+    bool open = true;
+    unsigned long long my_steps = 0;
+    unsigned my_esc_i = 0, my_esc_e = 0, my_lost = 0;
+
+    for (;;) {
+        const unsigned need = __ballot_sync(FULL, pid < 0);
+        if (need != 0u && open) {
+            const int leader = __ffs(need) - 1;
+            const int cnt = __popc(need);
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(k.queue, (unsigned long long)cnt);
+            base = __shfl_sync(FULL, base, leader);
+            if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
+            if (pid < 0) {
+                const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
+                if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
+                    pid = (long long)idx;
+                    const double xc = a.d_x[pid] / k.dx, yc = a.d_y[pid] / k.dx;
+                    ix = (int)xc;
+                    if (ix > nx - 1) ix = nx - 1;
+                    if (ix < 0) ix = 0;
+                    iy = (int)floor(yc);
+                    ox = (float)(xc - (double)ix);
+                    oy = (float)(yc - (double)iy);
+                    ox = ox >= 1.f ? ONE_BELOW : (ox < 0.f ? 0.f : ox);
+                    oy = oy >= 1.f ? ONE_BELOW : (oy < 0.f ? 0.f : oy);
+                    vx = (float)(a.d_vx[pid] / k.vscale);
+                    vy = (float)(a.d_vy[pid] / k.vscale);
+                    qm = (float)a.d_qm[pid];
+                    spc = a.d_spc[pid];
+                    steps = a.d_steps[pid];
+                    stop_at = min(a.max_steps, steps + a.step_budget);
+                }
+            }
+        }
+        if (__ballot_sync(FULL, pid >= 0) == 0u) {
+            if (!open) break;
+            continue;
+        }
+        if (pid < 0) continue;
+
+        // ---- field at the current position ----
+        int i0, i1, j0, j1;
+        float tx, ty;
+        if (ox >= 0.5f) { tx = ox - 0.5f; i0 = ix; i1 = ix + 1 == nx ? 0 : ix + 1; }
+        else { tx = ox + 0.5f; i0 = ix == 0 ? nx - 1 : ix - 1; i1 = ix; }
+        const int iyc = iy < 0 ? 0 : (iy > ny - 1 ? ny - 1 : iy);
+        if (oy >= 0.5f) { ty = oy - 0.5f; j0 = iyc; j1 = iy + 1 > ny - 1 ? ny - 1 : (iy + 1 < 0 ? 0 : iy + 1); }
+        else { ty = oy + 0.5f; j0 = iy - 1 < 0 ? 0 : (iy - 1 > ny - 1 ? ny - 1 : iy - 1); j1 = iyc; }
+        const tb_fcell c00 = F.at(i0 * ny + j0), c10 = F.at(i1 * ny + j0);
+        const tb_fcell c01 = F.at(i0 * ny + j1), c11 = F.at(i1 * ny + j1);
+        const float w00 = (1.f - tx) * (1.f - ty), w10 = tx * (1.f - ty);
+        const float w01 = (1.f - tx) * ty, w11 = tx * ty;
+        const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
+        const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
+        const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
+        const float inv_sw = 1.f / fmaxf(sw, 1e-12f);
+        const float ax = qm * (sex * inv_sw), ay = qm * (sey * inv_sw);
+
+        // ---- CFL step and trapezoid update ----
+        const float speed = sqrtf(vx * vx + vy * vy);
+        const float acc = sqrtf(ax * ax + ay * ay);
+        const float dt = cfl / (speed + sqrtf(2.f * acc) + k.inv_v);
+        const float vxn = vx + ax * dt, vyn = vy + ay * dt;
+        const float sx = 0.5f * (vx + vxn) * dt, sy = 0.5f * (vy + vyn) * dt;
+        const int ix0 = ix, iy0 = iy;
+        const float ox0 = ox, oy0 = oy;
+        ox += sx;
+        oy += sy;
+        int dix = 0, diy = 0;
+        if (ox >= 1.f) { ox -= 1.f; dix = 1; }
+        else if (ox < 0.f) { ox += 1.f; dix = -1; if (ox >= 1.f) ox = ONE_BELOW; }
+        if (oy >= 1.f) { oy -= 1.f; diy = 1; }
+        else if (oy < 0.f) { oy += 1.f; diy = -1; if (oy >= 1.f) oy = ONE_BELOW; }
+        ix = ix0 + dix;
+        ix = ix < 0 ? ix + nx : (ix >= nx ? ix - nx : ix);
+        iy = iy0 + diy;
+        vx = vxn; vy = vyn;
+        ++steps;
+        ++my_steps;
+
+        const bool escaped = iy >= ny;
+        const int iyn = iy < 0 ? 0 : iy;  // iy < ny here unless escaped
+        bool hit = !escaped && !F.vac(ix * ny + iyn);
+        int dcell = ix * ny + iyn;
+        if (!escaped && (hit ? first_face : (tapered && dix != 0))) {
+            // first solid face crossed (trench_charging_2d.py:512-539) in cell units
+            const int y0c = iy0 < 0 ? 0 : iy0;
+            const int diy_e = (iyn) - y0c;   // both rows clipped like the reference
+            if (hit || diy_e != 0) {
+                const float inf = __int_as_float(0x7f800000);
+                const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - ox0) / sx : inf;
+                const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - oy0) / sy : inf;
+                const bool x_first = fx < fy;
+                const int xn = ix;  // already wrapped ix0 + dix
+                const int ax_ = x_first ? xn : ix0, ay_ = x_first ? y0c : y0c + diy_e;
+                const bool use_last = dix != 0 && diy_e != 0 && F.vac(ax_ * ny + ay_);
+                const int cx = use_last ? xn : ax_, cy = use_last ? y0c + diy_e : ay_;
+                const bool face_x = use_last ? !x_first : x_first;
+                const int ccell = cx * ny + cy;
+                hit = !F.vac(ccell);
+                dcell = ccell;
+                if (hit && barrier) {
+                    const float4 b = __ldg(k.barrier + ccell);
+                    // neighbour the particle came from: W/E across an x face, S/N across a y face
+                    const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
+                    const float vn = face_x ? vx : vy;
+                    if (0.5f * vn * vn < qm * dphi) {
+                        if (face_x) vx = -vx; else vy = -vy;
+                        ix = ix0; iy = iy0; ox = ox0; oy = oy0;
+                        hit = false;
+                    }
+                }
+            }
+        }
+
+        int done = 0;
+        if (hit) {
+            if (dcell < 0 || dcell >= cells) {
+                atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BAD_CELL);
+            } else {
+                atomicAdd(a.d_counts + (size_t)spc * cells + dcell, 1);
+            }
+            if (a.d_hit) a.d_hit[pid] = dcell;
+            done = 1;
+        } else if (escaped) {
+            if (spc == 0) ++my_esc_i; else ++my_esc_e;
+            done = 2;
+        } else if (steps >= stop_at) {
+            if (steps >= a.max_steps) ++my_lost;
+            done = 3;
+        }
+        if (done) {
+            a.d_steps[pid] = steps;
+            if (done != 3) a.d_status[pid] = (int8_t)done;
+            if (done == 3 || a.write_state) {
+                a.d_x[pid] = ((double)ix + (double)ox) * k.dx;
+                a.d_y[pid] = ((double)iy + (double)oy) * k.dx;
+                a.d_vx[pid] = (double)vx * k.vscale;
+                a.d_vy[pid] = (double)vy * k.vscale;
+            }
+            pid = -1;
+        }
+    }
+
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        my_steps += __shfl_down_sync(FULL, my_steps, o);
+        my_esc_i += __shfl_down_sync(FULL, my_esc_i, o);
+        my_esc_e += __shfl_down_sync(FULL, my_esc_e, o);
+        my_lost += __shfl_down_sync(FULL, my_lost, o);
+    }
+    if (lane == 0) {
+        unsigned long long *t = reinterpret_cast<unsigned long long *>(a.d_totals);
+        if (my_esc_i) atomicAdd(t + 0, (unsigned long long)my_esc_i);
+        if (my_esc_e) atomicAdd(t + 1, (unsigned long long)my_esc_e);
+        if (my_lost) atomicAdd(t + 2, (unsigned long long)my_lost);
+        if (my_steps) atomicAdd(t + 3, my_steps);
+    }
+}
+
+// Packs FP64 fields into the FP32 tracer layout; one thread per cell.
+__global__ void pack_fields_kernel(int nx, int ny, double scale_e, double scale_phi, const uint8_t *vac,
+                                   const double *ex, const double *ey, const double *phi,
+                                   const double *wface, tb_fcell *out, float4 *bar, int padded) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cells = nx * ny;
+    if (c >= padded) return;
+    if (c >= cells) {
+        out[c] = tb_fcell{0.f, 0.f};
+        return;
+    }
+    const int v = vac[c] ? 1 : 0;
+    const float fx = (float)(ex[c] * (double)v * scale_e);
+    const float fy = (float)(ey[c] * (double)v * scale_e);
+    uint32_t bx = __float_as_uint(fx);
+    bx = v ? (bx | 1u) : (bx & ~1u);
+    out[c] = tb_fcell{__uint_as_float(bx), fy};
+    float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!v && phi != nullptr) {
+        const int ix = c / ny, iy = c - ix * ny;
+        const int w = (ix == 0 ? nx - 1 : ix - 1) * ny + iy;
+        const int e = (ix == nx - 1 ? 0 : ix + 1) * ny + iy;
+        const double f = wface[c], pc = phi[c];
+        b.x = (float)(f * (pc - phi[w]) * scale_phi);
+        b.y = (float)(f * (pc - phi[e]) * scale_phi);
+        b.z = iy > 0 ? (float)(f * (pc - phi[c - 1]) * scale_phi) : 0.f;
+        b.w = iy < ny - 1 ? (float)(f * (pc - phi[c + 1]) * scale_phi) : 0.f;
+    }
+    bar[c] = b;
+}
+
+}  // namespace
+
+int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
+                          const double *wface, double vscale, cudaStream_t s) {
+    const int cells = ctx->nx * ctx->ny;
+    const int padded = (cells + 1) & ~1;
+    const double scale_e = ctx->dx / (vscale * vscale);
+    const double scale_phi = 1.0 / (vscale * vscale);
+    const int threads = 256;
+    pack_fields_kernel<<<(padded + threads - 1) / threads, threads, 0, s>>>(
+        ctx->nx, ctx->ny, scale_e, scale_phi, ctx->d_vac, ex, ey, phi, wface, ctx->d_field, ctx->d_barrier,
+        padded);
+    TB_CUDA(ctx, cudaGetLastError());
+    ctx->vscale = vscale;
+    ctx->fields_ready = 1;
+    return TB_OK;
+}
+
+int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
+    K32 k;
+    k.a = *a;
+    k.nx = ctx->nx;
+    k.ny = ctx->ny;
+    k.dx = ctx->dx;
+    k.vscale = ctx->vscale;
+    k.inv_v = (float)(1.0 / ctx->vscale);
+    k.field = ctx->d_field;
+    k.barrier = ctx->d_barrier;
+    k.queue = ctx->d_queue;
+    k.err = ctx->d_err;
+    const int cells = ctx->nx * ctx->ny;
+    k.bytes = ((cells + 1) & ~1) * (int)sizeof(tb_fcell);
+    TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
+    int max_smem = 0;
+    TB_CUDA(ctx, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    const bool smem = k.bytes + 1024 <= max_smem;
+    long long want = (a->n + F32_THREADS - 1) / F32_THREADS;
+    int blocks = (int)(want < ctx->num_sms ? want : ctx->num_sms);
+    if (blocks < 1) blocks = 1;
+    if (smem) {
+        TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          k.bytes));
+        trace_f32_kernel<true><<<blocks, F32_THREADS, k.bytes, s>>>(k);
+    } else {
+        trace_f32_kernel<false><<<blocks, F32_THREADS, 0, s>>>(k);
+    }
+    TB_CUDA(ctx, cudaGetLastError());
+    return TB_OK;
+}

@@ -1,0 +1,258 @@
+"""B200Tracer: the reference tracer interface on the sm_100a kernels.
+
+``B200Tracer(vac, device)`` is called exactly like the reference
+``CudaTracer`` (trench_cuda.py:21-138) and ``trace_cpu``
+(trench_charging_2d.py:542):
+
+    cnt_i, cnt_e, escaped, lost = tracer(x, y, vx, vy, qm, spc, Ex, Ey, vac, p,
+                                         barrier=None, record=None, stop=None, rf=None)
+
+Inputs are host NumPy arrays (any memory order) or CUDA torch tensors; the
+outputs are new NumPy arrays.  ``precision="f32"`` runs the FP32 shared-memory
+kernel; ``"f64"`` runs the reference-exact FP64 kernel.  Trajectory recording
+and the RF in-flight clock always use the FP64 kernel.  There is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi
+from .params import is_tapered
+
+CHUNK_STEPS = 256      # step budget per launch when a stop event must be polled
+DEFAULT_VSCALE = 1e5   # m/s, velocity unit of the FP32 state
+
+
+def _validate_rf(rf, n, shape):
+    """trench_rf.py:21-32"""
+    if (not np.isfinite(rf["period"]) or rf["period"] <= 0
+            or not np.isfinite(rf["dt_max"]) or rf["dt_max"] <= 0):
+        raise ValueError("RF period and dt_max must be positive and finite")
+    for key in ("phi", "Ex", "Ey"):
+        if np.shape(rf[key]) != (2, *shape) or not np.isfinite(rf[key]).all():
+            raise ValueError("RF basis field has a wrong shape or non-finite values")
+    wave = np.asarray(rf["wave"])
+    if wave.ndim != 2 or wave.shape[1] != 2 or len(wave) < 2 or not np.isfinite(wave).all():
+        raise ValueError("RF voltage waveform is invalid")
+    if np.shape(rf["initial_time"]) != (n,) or not np.isfinite(rf["initial_time"]).all():
+        raise ValueError("particle launch times have a wrong shape or non-finite values")
+
+
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class Context:
+    """Owns one tb_ctx (one grid and vacuum mask on one device)."""
+
+    def __init__(self, vac, device=0, dx=1.0):
+        L = _capi.lib()
+        vac = np.ascontiguousarray(np.asarray(vac, dtype=bool), dtype=np.uint8)
+        self.nx, self.ny = vac.shape
+        h = ctypes.c_void_p()
+        code = L.tb_create(ctypes.byref(h), int(device), self.nx, self.ny, float(dx),
+                           vac.ctypes.data_as(ctypes.c_void_p))
+        if code == _capi.TB_ERR_DEVICE:
+            msg = L.tb_last_error(None).decode()
+            raise RuntimeError(f"{msg} (CUDA デバイス {device} は利用できません)")
+        _capi.raise_for(code, None)
+        self.handle = h
+        self.device = int(device)
+        buf = ctypes.create_string_buffer(128)
+        sms = ctypes.c_int()
+        L.tb_device_info(h, buf, 128, ctypes.byref(sms))
+        self.name = buf.value.decode()
+        self.num_sms = sms.value
+
+    def check(self, code):
+        _capi.raise_for(code, self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _capi.lib().tb_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class B200Tracer:
+    """Drop-in for ``CudaTracer`` (trench_cuda.py:21) running on the B200 kernels."""
+
+    def __init__(self, vac, device=0, precision="f32", vscale=DEFAULT_VSCALE):
+        if precision not in _capi.PRECISION:
+            raise ValueError(f"precision must be one of {tuple(_capi.PRECISION)}")
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device is visible (the B200 backend has no CPU path)")
+        self.vac = np.asarray(vac, dtype=bool).copy()
+        self.ctx = Context(self.vac, device)
+        self.device = self.ctx.device
+        self.name = self.ctx.name
+        self.precision = precision
+        self.vscale = float(vscale)
+        self.tdev = torch.device("cuda", self.device)
+        self.last = {}
+        self._ctx_dx = None
+
+    # -- helpers ---------------------------------------------------------------
+    def _dev(self, a, dtype):
+        if isinstance(a, torch.Tensor):
+            return a.to(device=self.tdev, dtype=dtype).contiguous()
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=_np_dtype(dtype))).to(self.tdev, non_blocking=False)
+
+    def _context_for(self, dx):
+        # The context stores dx; a tracer serves one geometry, dx comes from p.
+        if self._ctx_dx != dx:
+            self.ctx.close()
+            self.ctx = Context(self.vac, self.device, dx)
+            self._ctx_dx = dx
+        return self.ctx
+
+    # -- the reference call ------------------------------------------------------
+    def __call__(self, x, y, vx, vy, qm, spc, Ex, Ey, vac, p, barrier=None, record=None, stop=None, rf=None):
+        vac = np.asarray(vac)
+        if vac.shape != self.vac.shape or not np.array_equal(vac.astype(bool), self.vac):
+            raise ValueError("the tracer was built for another geometry; create a new tracer")
+        if not (0 < p.cfl <= 1) or p.max_steps < 1:
+            raise ValueError("CUDA tracing needs 0 < cfl <= 1 and max_steps >= 1")
+        n = len(x)
+        nx, ny = self.vac.shape
+        if any(np.shape(v) != (n,) for v in (x, y, vx, vy, qm, spc)):
+            raise ValueError("particle arrays differ in length")
+        if any(np.shape(v) != (nx, ny) for v in (Ex, Ey)):
+            raise ValueError("field shape does not match the grid")
+        spc_h = spc.cpu().numpy() if isinstance(spc, torch.Tensor) else np.asarray(spc)
+        if np.any((spc_h != 0) & (spc_h != 1)):
+            raise ValueError("species must be 0 (ion) or 1 (electron)")
+        if barrier is not None and any(np.shape(v) != (nx, ny) for v in barrier):
+            raise ValueError("wall potential shape does not match the grid")
+        if record is not None and p.probe_trajectories < 1:
+            raise ValueError("probe_trajectories must be at least 1")
+        if rf is not None:
+            _validate_rf(rf, n, self.vac.shape)
+        with torch.cuda.device(self.device):
+            return self._trace(x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf)
+
+    def _trace(self, x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf):
+        L = _capi.lib()
+        ctx = self._context_for(float(p.dx))
+        n = len(x)
+        nx, ny = self.vac.shape
+        f64, dev = torch.float64, self.tdev
+        precision = "f64" if (record is not None or rf is not None) else self.precision
+        stream = torch.cuda.current_stream(dev)
+        sp = ctypes.c_void_p(stream.cuda_stream)
+
+        X = [self._dev(v, f64).clone() for v in (x, y, vx, vy)]
+        QM = self._dev(qm, f64)
+        SPC = torch.from_numpy(np.ascontiguousarray(spc_h, dtype=np.int8)).to(dev)
+        EX, EY = self._dev(Ex, f64), self._dev(Ey, f64)
+        PHI = WF = None
+        if barrier is not None:
+            PHI, WF = self._dev(barrier[0], f64), self._dev(barrier[1], f64)
+        counts = torch.zeros((2, nx, ny), dtype=torch.int32, device=dev)
+        totals = torch.zeros(4, dtype=torch.int64, device=dev)
+        status = torch.full((n,), 3, dtype=torch.int8, device=dev)
+        hit = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        steps = torch.zeros(n, dtype=torch.int32, device=dev)
+
+        a = _capi.TraceArgs()
+        a.n = n
+        a.d_x, a.d_y, a.d_vx, a.d_vy = (_ptr(t) for t in X)
+        a.d_qm, a.d_spc = _ptr(QM), _ptr(SPC)
+        a.d_ex, a.d_ey = _ptr(EX), _ptr(EY)
+        a.d_phi, a.d_wface = _ptr(PHI), _ptr(WF)
+        a.max_steps = int(p.max_steps)
+        a.cfl = float(p.cfl)
+        a.tapered = int(is_tapered(p))
+        a.d_counts, a.d_totals = _ptr(counts), _ptr(totals)
+        a.d_status, a.d_hit, a.d_steps = _ptr(status), _ptr(hit), _ptr(steps)
+        a.write_state = int(record is not None)
+
+        keep = [X, QM, SPC, EX, EY, PHI, WF, counts, totals, status, hit, steps]
+        period = None
+        if rf is not None:
+            RFX, RFY, RFP = (self._dev(rf[k], f64) for k in ("Ex", "Ey", "phi"))
+            WAVE = self._dev(rf["wave"], f64)
+            period = float(rf["period"])
+            t0 = np.asarray(rf["initial_time"], dtype=np.float64) % period
+            CLOCK = torch.from_numpy(np.column_stack((t0, np.zeros(n)))).to(dev)
+            bound = np.abs(np.asarray(rf["wave"])).max(axis=0)
+            a.d_rf_ex, a.d_rf_ey, a.d_rf_phi, a.d_wave = _ptr(RFX), _ptr(RFY), _ptr(RFP), _ptr(WAVE)
+            a.n_phase = len(rf["wave"])
+            a.period, a.dt_max = period, float(rf["dt_max"])
+            a.bound_vs, a.bound_vm = float(bound[0]), float(bound[1])
+            a.d_clock = _ptr(CLOCK)
+            keep += [RFX, RFY, RFP, WAVE, CLOCK]
+        selected = None
+        if record is not None:
+            selected = np.unique(np.linspace(0, n - 1, min(p.probe_trajectories, n), dtype=int))
+            slots = np.full(n, -1, dtype=np.int32)
+            slots[selected] = np.arange(len(selected), dtype=np.int32)
+            stride = p.max_steps + 1
+            SLOTS = torch.from_numpy(slots).to(dev)
+            ENDP = torch.stack([X[0], X[1]], dim=1).contiguous()
+            PATHS = torch.zeros((max(len(selected), 1), stride, 2), dtype=f64, device=dev)
+            PLEN = torch.ones(max(len(selected), 1), dtype=torch.int32, device=dev)
+            if len(selected):
+                sel = torch.from_numpy(selected).to(dev)
+                PATHS[:len(selected), 0] = ENDP[sel]
+            a.record = 1
+            a.d_endpoints, a.d_slots, a.d_paths, a.d_path_len = _ptr(ENDP), _ptr(SLOTS), _ptr(PATHS), _ptr(PLEN)
+            a.path_stride = stride
+            keep += [SLOTS, ENDP, PATHS, PLEN]
+
+        if precision == "f32" and n:
+            self.ctx.check(L.tb_set_fields(ctx.handle, _ptr(EX), _ptr(EY), _ptr(PHI), _ptr(WF),
+                                           self.vscale, sp))
+        cancelled = False
+        if stop is None:
+            a.step_budget = int(p.max_steps)
+            if n:
+                ctx.check(L.tb_trace(ctx.handle, ctypes.byref(a), _capi.PRECISION[precision], sp))
+        else:
+            a.step_budget = min(CHUNK_STEPS, int(p.max_steps))
+            for _ in range(0, int(p.max_steps), CHUNK_STEPS):
+                if not n or not bool((status == 3).any()):
+                    break
+                if stop.is_set():
+                    cancelled = True
+                    break
+                ctx.check(L.tb_trace(ctx.handle, ctypes.byref(a), _capi.PRECISION[precision], sp))
+        ctx.check(L.tb_check(ctx.handle, sp))
+
+        cnt = counts.to(torch.int64).cpu().numpy()
+        tot = totals.cpu().numpy()
+        host_status = status.cpu().numpy()
+        escaped = np.array([tot[0], tot[1]], dtype=np.int64)
+        lost = int(np.count_nonzero(host_status == 3))
+        self.last = dict(particle_steps=int(tot[3]), status=host_status, hit=hit.cpu().numpy(),
+                         steps=steps.cpu().numpy(), precision=precision)
+        if record is not None:
+            host_hit = self.last["hit"]
+            cells = np.full((n, 2), -1, dtype=int)
+            ab = host_status == 1
+            cells[ab] = np.column_stack((host_hit[ab] // ny, host_hit[ab] % ny))
+            plen = PLEN.cpu().numpy()
+            paths = PATHS.cpu().numpy()
+            record.update(selected=selected, status=host_status, hit_cells=cells,
+                          initial_x=np.asarray(x).copy() if not isinstance(x, torch.Tensor) else x.cpu().numpy(),
+                          endpoints=ENDP.cpu().numpy(),
+                          final_velocity=np.column_stack((X[2].cpu().numpy(), X[3].cpu().numpy())),
+                          paths=[paths[k, :plen[k]].copy() for k in range(len(selected))],
+                          cancelled=cancelled or (stop is not None and stop.is_set()))
+            if rf is not None:
+                timing = CLOCK.cpu().numpy()
+                record.update(launch_phase=np.asarray(rf["initial_time"]) % period / period * 360,
+                              final_phase=timing[:, 0] / period * 360, flight_time=timing[:, 1])
+        del keep
+        return cnt[0], cnt[1], escaped, lost
+
+
+def _np_dtype(tdtype):
+    return {torch.float64: np.float64, torch.float32: np.float32, torch.int8: np.int8,
+            torch.int32: np.int32, torch.int64: np.int64, torch.uint8: np.uint8}[tdtype]
