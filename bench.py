@@ -1,0 +1,370 @@
+"""Benchmark of the per-batch charging step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: AR-8 RF-charging trench (60x250 cells of 5 nm, trench 20x160 with a
+2 deg taper, dielectric mask 20 cells eps_r 3 with a 5 deg taper), 2^19 ions +
+2^19 electrons per batch, bimodal ion energy distribution (Gaussians at 40 and
+140 eV, sigma 6 eV, equal weights), half-Gaussian angles (sigma 3 deg),
+electrons Te 3 eV, sheet leakage 1e-15 S, barrier wall model.  Synthetic,
+seeded inputs.  A step is one charging batch: trace -> deposit -> leakage ->
+potential -> field, on the device, replayed from a CUDA graph.
+
+value: traced particles per second over the timed steps (device-resident inputs,
+L2 flushed between steps, CUDA events).  e2e: the same through ChargingCase.load
++ step with the batch copied from pinned host memory every step and the history
+row read back.  Under torchrun every rank runs its own case (weak scaling, no
+collective on the data path); rank 0 prints the line.
+
+--impl reference times the reference algorithm on the host cores (the FP64 C
+restatement of the reference tracer plus the NumPy/SciPy batch update) on a
+bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from dataclasses import replace
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "traced particles/s and batches/s on 1 B200 at <=1% flux error vs plain FP64 form"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def workload(n_per_species=1 << 19):
+    from trench_b200.params import Params
+    return replace(Params(), nx=60, trench_w=20, trench_d=160, floor_t=10, mask_t=20, n_vac=60,
+                   trench_taper_deg=2.0, mask_taper_deg=5.0, mask_type="dielectric", mask_eps_r=3.0,
+                   electron_temp_eV=3.0, bias="rf", field_mode="floating", sigma_s=1e-15,
+                   n_per_batch=n_per_species, seed=1)
+
+
+def ion_sampler(p):
+    from trench_b200 import inject
+    energy = inject.mixture_energy([(0.5, "normal", 40.0, 6.0), (0.5, "normal", 140.0, 6.0)])
+    return inject.energy_angle_sampler(p, energy, inject.half_gaussian_angle(3.0))
+
+
+def config(p, extra=None):
+    c = {"workload": "AR-8 RF-charging trench, 60x250 cells, 2^20 particles/batch, bimodal IED 40/140 eV, "
+                     "half-Gaussian IAD 3 deg, Te 3 eV, leakage 1e-15 S, barrier walls",
+         "grid": [p.nx, p.floor_t + p.trench_d + p.mask_t + p.n_vac], "particles_per_batch": 2 * p.n_per_batch,
+         "max_steps": p.max_steps, "cfl": p.cfl}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in Path(self.path).read_text().splitlines():
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def profile_traffic():
+    """DRAM bytes per particle of the FP32 tracer from the committed ncu summary, if any."""
+    try:
+        d = json.loads((ROOT / "profiles" / "trace_f32_traffic.json").read_text())
+        return float(d["dram_bytes_per_particle"]), float(d.get("dram_bytes_per_step", 0.0))
+    except Exception:
+        return None
+
+
+def cpu_baseline(p, sample_per_species, seconds_budget=20.0):
+    """The oracle (FP64 C restatement of the reference tracer, all host threads) plus the
+    oracle batch update, on a bounded sample of this workload."""
+    from oracle import oracle_fields as OF
+    from oracle import oracle_trace as OT
+    from trench_b200 import geometry, inject
+    threads = OT.default_threads()
+    q = replace(p, n_per_batch=sample_per_species)
+    solid, mask, _, _ = geometry.build_geometry(q)
+    st = OF.BatchState(q, solid, mask)
+    rng = np.random.default_rng(7)
+    sampler = ion_sampler(q)
+    done, t_total, batches = 0, 0.0, 0
+    while t_total < seconds_budget and batches < 50:
+        parts = inject.inject(q, q.n_per_batch, solid.shape[1], rng, ion_velocity=sampler)
+        t0 = time.perf_counter()
+        out = OT.trace(*parts, st.Ex, st.Ey, ~solid, q, st.barrier(), threads=threads)
+        st.step(*out)
+        t_total += time.perf_counter() - t0
+        done += 2 * q.n_per_batch
+        batches += 1
+    return {"value": done / t_total, "unit": "particles/s", "cores": threads, "kind": "port",
+            "sample": f"{batches} batches of {2 * sample_per_species} particles (same geometry and "
+                      f"distributions, {sample_per_species} per species), trace + batch update, "
+                      f"{t_total:.1f} s", "batches_per_s": batches / t_total}
+
+
+def run_reference(args, p):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sample = 1 << 13
+    steps = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(p, sample, seconds_budget=8.0 if i >= args.warmup else 2.0)
+        if i >= args.warmup:
+            steps.append(b)
+        base = b
+    value = float(np.mean([s["value"] for s in steps]))
+    ms = 1000.0 * 2 * sample / value
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": config(p, {"sample_particles_per_step": 2 * sample}),
+            "cpu_baseline": {**base, "value": value},
+            "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, p):
+    import torch
+    import torch.distributed as dist
+    from trench_b200 import inject
+    from trench_b200.step import ChargingCase
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    n_steps = args.warmup + args.steps
+    case = ChargingCase(replace(p, seed=p.seed + rank), device=local, precision="f32", green="f64",
+                        max_batches=2 * n_steps + 8)
+    ny = case.ny
+    sampler = ion_sampler(p)
+    rng = np.random.default_rng(100 + rank)
+    pool_n = min(n_steps, 6)
+    host = []
+    for _ in range(pool_n):
+        parts = inject.inject(p, p.n_per_batch, ny, rng, ion_velocity=sampler)
+        host.append([torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in parts])
+    dev_pool = [[t.to(dev) for t in h] for h in host]
+    n = 2 * p.n_per_batch
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    # graph with externally visible timing events around the tracer kernel
+    t0e = torch.cuda.Event(enable_timing=True, external=True)
+    t1e = torch.cuda.Event(enable_timing=True, external=True)
+    case.load(*dev_pool[0])
+    case.step()                               # eager first batch (warm-up 1)
+    torch.cuda.synchronize()
+    case.trace_events = (t0e, t1e)
+    graph_ok = True
+    try:
+        case.capture(n)
+    except Exception as exc:  # noqa: BLE001
+        graph_ok = False
+        print(f"# CUDA graph capture failed, timing eager launches: {exc}", file=sys.stderr)
+
+    def one_step(i):
+        src = dev_pool[i % pool_n]
+        for dst, s in zip(case.X + [case.SPC], src):
+            dst[:n].copy_(s)
+        if graph_ok:
+            case.replay()
+        else:
+            case.step(n)
+
+    for i in range(1, args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    clocks = Clocks(local)
+    clocks.start()
+    steps_before = case.batches_done()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    trace_ms = []
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        src = dev_pool[(args.warmup + k) % pool_n]
+        for dst, s in zip(case.X + [case.SPC], src):
+            dst[:n].copy_(s)
+        starts[k].record()
+        if graph_ok:
+            case.replay()
+        else:
+            case.step(n)
+        ends[k].record()
+        flush.zero_()
+        ends[k].synchronize()
+        trace_ms.append(t0e.elapsed_time(t1e))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - wall0
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    hist = case.history()
+    steps_per_batch = hist["particle_steps"][steps_before:steps_before + args.steps]
+
+    # e2e: host buffers through the public API (H2D each step, history row D2H)
+    e2e_ms = []
+    row = torch.empty(case.hist_cols, dtype=torch.float64).pin_memory()
+    for k in range(args.steps):
+        h = host[k % pool_n]
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        case.load(*h, non_blocking=True)
+        if graph_ok:
+            case.replay()
+        else:
+            case.step(n)
+        b = case.batches_done() - 1 if False else None  # noqa: F841
+        row.copy_(case.hist[min(steps_before + args.steps + k, case.max_batches - 1)], non_blocking=True)
+        s1.record()
+        flush.zero_()
+        s1.synchronize()
+        e2e_ms.append(s0.elapsed_time(s1))
+    clk = clocks.stop()
+    case.check()
+    h2d = sum(t.numel() * t.element_size() for t in host[0])
+    d2h = row.numel() * row.element_size()
+    e2e_total = float(sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    if rank != 0:
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    particles = n * args.steps * world
+    value = particles / (total_ms / 1000.0)
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    # Tracer roofline: algorithmic bytes = 36 B per particle-step (4 bilinear corners of
+    # Ex, Ey, vacuum in FP32) + 28 B per particle (SoA load + status/hit store).
+    alg_bytes = [36.0 * s + 28.0 * n for s in steps_per_batch]
+    achieved = float(np.mean([b / (t / 1000.0) for b, t in zip(alg_bytes, trace_ms)])) / 1e9
+    smem_peak = case_smem_peak(case)
+    traffic = profile_traffic()
+    mean_steps = float(np.mean(steps_per_batch))
+    roof = {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+            "frac": achieved / smem_peak if smem_peak else None,
+            "peak_source": "measured shared-memory load bandwidth (bench microkernel)",
+            "traffic": (traffic[0] * n + traffic[1] * mean_steps) if traffic else None,
+            "hbm_peak_gbs": hbm, "hbm_frac_of_measured": (achieved / hbm) if hbm else None,
+            "kernel": "trace_f32_kernel", "trace_ms_per_launch": float(np.mean(trace_ms)),
+            "particle_steps_per_launch": mean_steps,
+            "particle_steps_per_s": float(np.mean([s / (t / 1000.0) for s, t in zip(steps_per_batch, trace_ms)]))}
+    cpu = cpu_baseline(p, 1 << 15, seconds_budget=float(os.environ.get("TB_CPU_SECONDS", "15")))
+    line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(p, {"l2": "flushed between timed steps (256 MiB write)",
+                                 "graph": graph_ok, "precision": "f32 tracer, f64 Green's operator, "
+                                 "f64 charge/leakage/conductor", "parallelism": f"{world} independent cases"}),
+            "batches_per_s": 1000.0 * args.steps * world / total_ms,
+            "e2e": {"value": particles / (e2e_total / 1000.0), "unit": "particles/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "batches_per_s": 1000.0 * args.steps * world / e2e_total},
+            "gpu_launches": 10 * args.steps,
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
+            "wall_s": wall}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def case_smem_peak(case):
+    """Shared-memory load bandwidth measured on this GPU (GB/s)."""
+    import ctypes
+    from trench_b200 import _capi
+    out = ctypes.c_double()
+    code = _capi.lib().tb_bench_smem(case.ctx.handle, ctypes.byref(out))
+    return out.value if code == 0 else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    p = workload()
+    if args.impl == "reference":
+        return run_reference(args, p)
+    return run_b200(args, p)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

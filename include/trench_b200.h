@@ -65,8 +65,8 @@ typedef struct {
     int path_stride;
     /* outputs */
     int32_t *d_counts;               /* (2, nx, ny) hit histogram per species, accumulated */
-    int64_t *d_totals;               /* [4] escaped ions, escaped electrons, lost, particle-steps;
-                                        accumulated */
+    int64_t *d_totals;               /* [8] escaped ions, escaped electrons, lost, particle-steps,
+                                        absorbed ions, absorbed electrons, -, -; accumulated */
     int8_t *d_status;                /* (n) 1 absorbed, 2 escaped, 3 live; in/out, required */
     int32_t *d_hit;                  /* (n) absorbing cell or -1; optional */
     int32_t *d_steps;                /* (n) steps taken; in/out, required */
@@ -101,6 +101,78 @@ int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the
  * grid, a bulk copy that did not complete in its bounded wait). */
 int tb_check(tb_ctx *ctx, void *stream);
+
+/* ---- Poisson: multigrid-preconditioned CG ------------------------------------
+ * Operator L = -dx^2 A, the SPD form of the reference's 5-point matrix
+ * (trench_charging_2d.py:252-294): per cell the diagonal d > 0 and the
+ * couplings kE (to ix+1, periodic) and kN (to iy+1) >= 0, host arrays of nx*ny.
+ * Cells with h_fixed != 0 are Dirichlet zero.  Replaces the SuperLU factorisation
+ * and solve of make_solver / setup_fields (trench_charging_2d.py:297-309, 378-392). */
+int tb_poisson_setup(tb_ctx *ctx, const double *h_diag, const double *h_ke, const double *h_kn,
+                     const uint8_t *h_fixed, int max_rhs);
+/* Number of multigrid levels built by tb_poisson_setup (0 before setup). */
+int tb_poisson_levels(const tb_ctx *ctx);
+/* Solve L x = b for nrhs right-hand sides, d_b and d_x (nrhs, nx*ny) FP64; d_x is
+ * the initial guess on entry.  b must be zero on fixed cells.  Stops when every
+ * relative residual |b - L x| / |b| <= rtol, after at most max_outer FP64
+ * refinement steps of `inner` FP32 PCG iterations each.  Synchronises `stream`
+ * once per refinement step.  TB_ERR_CONVERGENCE if rtol is not reached. */
+int tb_poisson_solve(tb_ctx *ctx, int nrhs, const double *d_b, double *d_x, double rtol, int max_outer,
+                     int inner, int *iters, double *h_resid, void *stream);
+
+/* ---- Per-batch charge and field update ------------------------------------------
+ * The state is the charge density on the m surface cells (charge is only ever
+ * deposited there); the potential is phi = external + G rho_s with G the surface
+ * Green's operator built once with tb_poisson_solve.  Together the two calls
+ * replace the body of the reference batch loop after the trace
+ * (trench_charging_2d.py:1239-1285). */
+#define TB_SFLAG_COND 1u     /* surface cell is a conductor cell */
+#define TB_SFLAG_REGION 2u   /* counted in the leakage current monitor */
+#define TB_SFLAG_BOTTOM 4u   /* bottom row (floor_t-1) inside the bottom opening */
+
+typedef struct {
+    int m;                           /* surface cells */
+    const int32_t *d_surf;           /* (m) flat cell index */
+    const uint8_t *d_sflag;          /* (m) TB_SFLAG_* bits */
+    double *d_rho_s;                 /* (m) charge density, C/m^3 (state) */
+    double *d_rho_prev;              /* (m) scratch */
+    double *d_work;                  /* (2m) scratch */
+    const double *d_leak_M;          /* (m, m) implicit leakage operator, NULL = no leakage */
+    const double *d_leak_h;          /* (m) dt G phi_ext on surface cells, or NULL */
+    const double *d_g_s;             /* (m) floating-conductor response at surface cells, or NULL */
+    int c_slot;                      /* surface index holding the floating conductor's charge, or -1 */
+    int floating, driven;
+    double q_macro, dx, C_cond, Te, dt_batch, leak_norm, bottom_norm, n_per_batch;
+    int n_rows;                      /* cells whose potential is needed (vacuum + surface) */
+    const int32_t *d_rows;           /* (n_rows) flat cell index */
+    const float *d_green;            /* (n_rows, m) FP32 Green's operator, or NULL */
+    const double *d_green64;         /* (n_rows, m) FP64 Green's operator, or NULL */
+    const double *d_ext;             /* (nx*ny) external potential */
+    double *d_phi;                   /* (nx*ny) potential; rows are rewritten each batch */
+    double *d_ex, *d_ey;             /* (nx*ny) FP64 field, or NULL */
+    const double *d_wface;           /* (nx*ny) wall barrier weight, NULL = absorb model */
+    double v_sub, v_top;             /* ghost-cell voltages of the field (trench_charging_2d.py:446-447) */
+    int top_dirichlet;
+    double vscale;                   /* velocity unit of the FP32 tracer state, m/s */
+    double *d_hist;                  /* (max_batches, hist_cols): ratio_i, ratio_e, esc_e, lost, leak,
+                                        particle-steps, probe potentials... */
+    int hist_cols, max_batches;
+    int n_probes;
+    const int32_t *d_probes;         /* (n_probes) flat cell index */
+    int32_t *d_batch;                /* device batch counter (start at -1) */
+    const int32_t *d_counts;         /* (2, nx*ny) tracer counts of this batch */
+    const int64_t *d_totals;         /* tracer totals of this batch */
+} tb_step_desc;
+
+/* Deposit, leakage, conductor step and history scalars (one batch). */
+int tb_step_charge(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
+/* Potential on the needed cells, FP64 field, packed FP32 tracer field (as
+ * tb_set_fields) and probe history. */
+int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
+
+/* Measured shared-memory load bandwidth of the context's GPU (GB/s, all SMs, 8-byte
+ * loads like the FP32 tracer's gathers).  A benchmark helper; synchronises the device. */
+int tb_bench_smem(tb_ctx *ctx, double *gbs);
 
 #ifdef __cplusplus
 }

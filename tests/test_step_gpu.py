@@ -1,0 +1,152 @@
+"""Multigrid solver and device batch loop against the reference (golden fixtures) and the oracle.
+
+Mirrors the reference's own checks: Poisson solutions (tests/test_features.py:39-49,
+65-76), leakage conservation (tests/test_taper.py:112-130) and whole-run CPU/CUDA
+agreement (tests/test_cuda.py:106-119).
+"""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import oracle_fields as OF
+from oracle import oracle_trace as OT
+from trench_b200 import geometry, inject
+from trench_b200.params import EPS0, Params
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case_cls(cuda_device):
+    from trench_b200.step import ChargingCase
+    return ChargingCase
+
+
+@pytest.mark.parametrize("name", ["floating", "fixed", "dielectric", "cfg2"])
+def test_solver_matches_reference_lu(case_cls, name):
+    """Potential of a given charge: multigrid vs the reference's LU within 1e-9 V
+    (north-star bar 1e-3 V); leakage operator and conductor response likewise."""
+    g = load_golden(f"fields_{name}.npz")
+    p = g["p"]
+    case = case_cls(replace(p, n_batches=1), green="f64")
+    np.testing.assert_allclose(case.external, g["external"], rtol=0, atol=1e-9)
+    phi = case.solver.solve((-g["rho"] / EPS0).ravel()).reshape(g["rho"].shape) + case.external
+    np.testing.assert_allclose(phi, g["phi"], rtol=0, atol=1e-9)
+    np.testing.assert_array_equal(case.S, g["leak_flat"])
+    M = case.leak_M.cpu().numpy()
+    if "leak_M" in g:
+        np.testing.assert_allclose(M, g["leak_M"], rtol=0, atol=1e-10)
+    else:
+        q = np.random.default_rng(11).normal(size=(case.m, 4))
+        np.testing.assert_allclose(M @ q, g["leak_MQ"], rtol=1e-10, atol=1e-10)
+    # leakage conserves charge (tests/test_taper.py:119-125)
+    np.testing.assert_allclose(M.sum(axis=0), 1.0, rtol=0, atol=1e-9)
+    if "g_cond" in g:
+        np.testing.assert_allclose(case.g_cond, g["g_cond"], rtol=1e-9, atol=0)
+        assert case.C_cond == pytest.approx(float(g["C_cond"]), rel=1e-9)
+
+
+@pytest.mark.parametrize("name", ["floating", "dielectric", "cfg2"])
+def test_green_operator_reproduces_solve(case_cls, name):
+    """phi = external + G rho_s on every row cell, for an arbitrary surface charge."""
+    g = load_golden(f"fields_{name}.npz")
+    p = g["p"]
+    for green, tol in (("f64", 1e-9), ("f32", 1e-4)):
+        case = case_cls(replace(p, n_batches=1), green=green)
+        import torch
+        case.rho_s.copy_(torch.from_numpy(g["rho"].ravel()[case.S]))
+        case._potential()
+        got = case.phi.cpu().numpy()[case.rows]
+        np.testing.assert_allclose(got, g["phi"].ravel()[case.rows], rtol=0, atol=tol)
+        ex, ey = case.fields()
+        if green == "f64":
+            np.testing.assert_allclose(ex, g["Ex"], rtol=1e-9, atol=1.0)
+            np.testing.assert_allclose(ey, g["Ey"], rtol=1e-9, atol=1.0)
+        else:
+            # FP32 storage of G: the field carries FP32 noise, bounded relative to the field scale
+            scale = max(np.abs(g["Ex"]).max(), np.abs(g["Ey"]).max())
+            assert np.abs(ex - g["Ex"]).max() <= 1e-4 * scale
+            assert np.abs(ey - g["Ey"]).max() <= 1e-4 * scale
+
+
+def test_solver_linear_profile_in_homogeneous_medium(case_cls):
+    """trench tests/test_features.py:39-49: Dirichlet potentials give a linear profile."""
+    from trench_b200.fields import FieldSolver
+    from trench_b200.tracer import Context
+    p = replace(Params(), nx=20, trench_w=6, trench_d=12, floor_t=4, mask_t=4, n_vac=8, bias="dc",
+                field_mode="fixed", substrate_voltage=-12, top_voltage=8)
+    solid = np.zeros((p.nx, 25), dtype=bool)
+    ctx = Context(~solid, 0, p.dx)
+    s = FieldSolver(ctx, p, np.ones(solid.shape), np.zeros_like(solid), True)
+    from trench_b200.fields import boundary_rhs
+    ext = s.solve(boundary_rhs(p, np.ones(solid.shape), dict(substrate=-12, top=8, mask=0)).ravel())
+    y = (np.arange(25) + 0.5) / 25
+    np.testing.assert_allclose(ext.reshape(solid.shape), np.broadcast_to(-12 + 20 * y, solid.shape), atol=1e-10)
+
+
+@pytest.mark.parametrize("name", ["floating_leak", "floating_noleak", "fixed_leak", "dielectric_leak",
+                                  "absorb_leak", "taper_leak"])
+def test_fp64_batch_loop_matches_reference_run(case_cls, name):
+    """FP64 tracer + FP64 Green's operator: the reference run() to 1e-10 relative
+    (the reference's own CPU/CUDA bar, tests/test_cuda.py:114-119)."""
+    g = load_golden(f"run_{name}.npz")
+    p = g["p"]
+    case = case_cls(p, precision="f64", green="f64")
+    res = case.run()
+    np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(res["mean_phi"], g["mean_phi"], rtol=1e-10, atol=1e-8)
+    for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
+        np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])
+    np.testing.assert_allclose(res["hist"]["leak"], g["hist_leak"], rtol=1e-9, atol=1e-12)
+    for k in case.probes:
+        np.testing.assert_allclose(res["hist"][k], g[f"hist_{k}"], rtol=1e-10, atol=1e-8)
+
+
+def test_fp32_batch_loop_tracks_oracle(case_cls):
+    """FP32 tracer + FP64 Green's operator over 5 batches of the AR-8 geometry with
+    2^14 particles per species: bottom ion flux within 3 sigma of the FP64 oracle
+    batch loop fed the same injected particles, potentials within 1% of the swing."""
+    p = replace(Params(), nx=60, trench_w=20, trench_d=160, floor_t=10, mask_t=20, n_vac=60, trench_taper_deg=2.0,
+                mask_taper_deg=5.0, mask_type="dielectric", mask_eps_r=3.0, electron_temp_eV=3.0, bias="dc",
+                ion_energy_eV=90.0, n_per_batch=1 << 14, n_batches=5, seed=3)
+    case = case_cls(p, precision="f32", green="f64")
+    res = case.run()
+    solid, mask, _, _ = geometry.build_geometry(p)
+    st = OF.BatchState(p, solid, mask)
+    rng = np.random.default_rng(p.seed)
+    for _ in range(p.n_batches):
+        parts = inject.inject(p, p.n_per_batch, solid.shape[1], rng)
+        st.step(*OT.trace(*parts, st.Ex, st.Ey, ~solid, p, st.barrier()))
+    ri, ro = res["hist"]["ratio_i_bottom"], np.array(st.hist["ratio_i_bottom"])
+    norm = p.n_per_batch * (case.b1 - case.b0) / p.nx
+    sigma = np.sqrt(np.maximum(ro * norm, 1)) / norm
+    assert np.all(np.abs(ri - ro) <= 3 * sigma + 1e-12), (ri, ro)
+    swing = np.ptp(st.phi)
+    assert np.max(np.abs(res["mean_phi"] - st.phi)) <= 0.01 * swing
+
+
+def test_graph_replay_equals_eager(case_cls):
+    """A captured batch replays the same kernels: same counts as an eager batch."""
+    import torch
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc",
+                sigma_s=1e-14, n_per_batch=2000, n_batches=4)
+    a = case_cls(p, precision="f32")
+    b = case_cls(p, precision="f32")
+    parts = inject.inject(p, p.n_per_batch, a.ny, np.random.default_rng(9))
+    a.load(*parts)
+    b.load(*parts)
+    a.step()
+    b.capture()
+    torch.cuda.synchronize()
+    # capture ran nothing; replays do the work
+    for _ in range(2):
+        a.load(*parts)
+        a.step()
+    b.replay()
+    b.replay()
+    b.replay()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(a.rho(), b.rho())
+    np.testing.assert_array_equal(a.history()["ratio_i_bottom"], b.history()["ratio_i_bottom"])

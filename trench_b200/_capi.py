@@ -48,6 +48,32 @@ class TraceArgs(ctypes.Structure):
     ]
 
 
+class StepDesc(ctypes.Structure):
+    """Mirror of ``tb_step_desc``."""
+    _fields_ = [
+        ("m", ctypes.c_int),
+        ("d_surf", _vp), ("d_sflag", _vp),
+        ("d_rho_s", _vp), ("d_rho_prev", _vp), ("d_work", _vp),
+        ("d_leak_M", _vp), ("d_leak_h", _vp), ("d_g_s", _vp),
+        ("c_slot", ctypes.c_int),
+        ("floating", ctypes.c_int), ("driven", ctypes.c_int),
+        ("q_macro", _dbl), ("dx", _dbl), ("C_cond", _dbl), ("Te", _dbl), ("dt_batch", _dbl),
+        ("leak_norm", _dbl), ("bottom_norm", _dbl), ("n_per_batch", _dbl),
+        ("n_rows", ctypes.c_int),
+        ("d_rows", _vp), ("d_green", _vp), ("d_green64", _vp), ("d_ext", _vp), ("d_phi", _vp),
+        ("d_ex", _vp), ("d_ey", _vp), ("d_wface", _vp),
+        ("v_sub", _dbl), ("v_top", _dbl),
+        ("top_dirichlet", ctypes.c_int),
+        ("vscale", _dbl),
+        ("d_hist", _vp),
+        ("hist_cols", ctypes.c_int), ("max_batches", ctypes.c_int),
+        ("n_probes", ctypes.c_int),
+        ("d_probes", _vp), ("d_batch", _vp), ("d_counts", _vp), ("d_totals", _vp),
+    ]
+
+
+SFLAG_COND, SFLAG_REGION, SFLAG_BOTTOM = 1, 2, 4
+
 # Every symbol the header declares, with its ctypes signature.
 SIGNATURES = {
     "tb_version": (ctypes.c_int, []),
@@ -58,6 +84,13 @@ SIGNATURES = {
     "tb_set_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _vp]),
     "tb_trace": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs), ctypes.c_int, _vp]),
     "tb_check": (ctypes.c_int, [_vp, _vp]),
+    "tb_poisson_setup": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int]),
+    "tb_poisson_levels": (ctypes.c_int, [_vp]),
+    "tb_poisson_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _dbl, ctypes.c_int, ctypes.c_int,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_dbl), _vp]),
+    "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
+    "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
+    "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
 }
 
 _lib = None

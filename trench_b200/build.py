@@ -22,6 +22,9 @@ UNITS = {
     "tb_capi.cu": [],
     "tb_trace_f64.cu": ["-fmad=false"],
     "tb_trace_f32.cu": [],
+    "tb_poisson.cu": [],
+    "tb_step.cu": ["-fmad=false"],
+    "tb_bench.cu": [],
 }
 
 

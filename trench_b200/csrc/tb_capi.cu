@@ -34,6 +34,7 @@ static int release(tb_ctx *c) {
     cudaFree(c->d_barrier);
     cudaFree(c->d_queue);
     cudaFree(c->d_err);
+    tb_poisson_free(c->poisson);
     if (prev >= 0) cudaSetDevice(prev);
     delete c;
     return TB_OK;
@@ -63,6 +64,7 @@ extern "C" int tb_create(tb_ctx **out, int device, int nx, int ny, double dx, co
     }
     snprintf(c->name, sizeof(c->name), "%.120s", prop.name);
     c->num_sms = prop.multiProcessorCount;
+    c->max_smem = (int)prop.sharedMemPerBlockOptin;
     const size_t cells = (size_t)nx * ny;
     const size_t padded = (cells + 1) & ~(size_t)1;
     e = cudaMalloc(&c->d_vac, cells);
@@ -75,6 +77,11 @@ extern "C" int tb_create(tb_ctx **out, int device, int nx, int ny, double dx, co
     if (e == cudaSuccess) e = cudaMemset(c->d_barrier, 0, padded * sizeof(float4));
     if (e != cudaSuccess) {
         tb_cuda_check(nullptr, e, "tb_create allocation");
+        release(c);
+        return TB_ERR_CUDA;
+    }
+    if (tb_configure_trace_f32(c) != TB_OK) {
+        tb_fail(nullptr, TB_ERR_CUDA, "%s", c->err);
         release(c);
         return TB_ERR_CUDA;
     }
@@ -110,7 +117,9 @@ static int check_device_flag(tb_ctx *ctx, cudaStream_t s) {
     if (flag != TB_DERR_NONE) {
         TB_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
         return tb_fail(ctx, TB_ERR_KERNEL, "kernel check failed (code %d: %s)", flag,
-                       flag == TB_DERR_BULK_TIMEOUT ? "bulk copy wait gave up" : "deposit cell out of range");
+                       flag == TB_DERR_BULK_TIMEOUT   ? "bulk copy wait gave up"
+                       : flag == TB_DERR_BAD_CELL   ? "deposit cell out of range"
+                                                    : "absorbed particle outside the surface cells");
     }
     return TB_OK;
 }

@@ -12,11 +12,15 @@
 #define TB_DERR_NONE 0
 #define TB_DERR_BULK_TIMEOUT 1   // bounded wait on a bulk-copy barrier gave up
 #define TB_DERR_BAD_CELL 2       // a deposit cell fell outside the grid
+#define TB_DERR_OFF_SURFACE 3    // an absorbed particle was counted outside the surface cells
 
 // Packed FP32 field cell: E*vac in cell units; bit 0 of .x carries the vacuum flag.
 struct __align__(8) tb_fcell {
     float ex, ey;
 };
+
+struct tb_poisson;
+void tb_poisson_free(tb_poisson *ps);
 
 struct tb_ctx {
     int device = 0;
@@ -31,6 +35,9 @@ struct tb_ctx {
     int *d_err = nullptr;                // scratch: device error flag
     double vscale = 1e5;                 // velocity unit of the FP32 state, m/s
     int fields_ready = 0;
+    int max_smem = 0;                    // opt-in shared memory per block (bytes)
+    int smem_attr_bytes = 0;             // dynamic shared memory set on the FP32 tracer
+    tb_poisson *poisson = nullptr;        // multigrid hierarchy (tb_poisson_setup)
     char err[512] = {0};
 };
 
@@ -48,6 +55,7 @@ int tb_cuda_check(tb_ctx *ctx, cudaError_t e, const char *what);
 // Launchers implemented per translation unit.
 int tb_launch_trace_f64(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s);
 int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s);
+int tb_configure_trace_f32(tb_ctx *ctx);
 int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
                           const double *wface, double vscale, cudaStream_t s);
 

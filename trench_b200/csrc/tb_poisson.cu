@@ -1,0 +1,487 @@
+// Geometric-multigrid-preconditioned CG for the staircase Poisson operator.
+//
+// Replaces the reference's SuperLU factorisation (trench_charging_2d.py:297-309,
+// 378-392).  The operator is the SPD form L = -dx^2 * A of the reference's
+// 5-point finite-volume matrix A (trench_charging_2d.py:252-294): per cell a
+// diagonal d > 0 and non-negative couplings kE (to the east neighbour, x
+// periodic) and kN (to the north neighbour).  Cells marked fixed are Dirichlet
+// zero (identity rows, couplings into them removed) -- a driven or, with the
+// superposition done by the caller, a floating conductor.
+//
+// Precision: FP32 V-cycles inside an FP32 PCG, wrapped in FP64 iterative
+// refinement (residual r = b - L x in FP64, normalised before each FP32 solve).
+//
+// Hierarchy: cell-centred 2x2 aggregation; the coarse operator is one half of
+// the Galerkin product P^T L P for piecewise-constant P restricted to free
+// cells (the scaling that makes aggregation consistent with rediscretisation).
+// Smoother: red-black Gauss-Seidel, forward before and reversed after the
+// coarse correction, so the V-cycle is a symmetric preconditioner.
+//
+// Many right-hand sides are solved together: vectors are (nrhs, cells) and
+// every kernel covers all of them in one launch (blockIdx.y = rhs).
+#include <math.h>
+
+#include <vector>
+
+#include "tb_internal.cuh"
+
+namespace {
+
+constexpr int PT = 256;  // threads per block
+
+struct Level {
+    int nx = 0, ny = 0;
+    int n = 0;
+    float *d = nullptr, *ke = nullptr, *kn = nullptr;
+    uint8_t *fixed = nullptr;
+    float *x = nullptr, *b = nullptr, *r = nullptr;  // (max_rhs, n)
+};
+
+}  // namespace
+
+struct tb_poisson {
+    int max_rhs = 0;
+    std::vector<Level> lev;
+    double *d64 = nullptr, *ke64 = nullptr, *kn64 = nullptr;
+    double *r64 = nullptr;                     // (max_rhs, n)
+    float *e = nullptr, *pr = nullptr, *pz = nullptr, *pp = nullptr, *pq = nullptr;  // PCG vectors
+    double *scal = nullptr;                    // (max_rhs, 8) per-rhs scalars
+    int pre = 1, post = 1, coarse_sweeps = 16;
+};
+
+namespace {
+
+enum { S_RR = 0, S_BB = 1, S_RZ = 2, S_PQ = 3, S_RZ_NEW = 4, S_NORM = 5 };
+
+__device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
+
+// y = L x at one cell (FP32 or FP64 operator)
+template <typename T, typename V>
+__device__ __forceinline__ V apply_at(const T *d, const T *ke, const T *kn, const V *x, int nx, int ny, int c) {
+    const int ix = c / ny, iy = c - ix * ny;
+    const int w = wrapx(ix - 1, nx) * ny + iy, e = wrapx(ix + 1, nx) * ny + iy;
+    V s = (V)d[c] * x[c] - (V)ke[c] * x[e] - (V)ke[w] * x[w];
+    if (iy + 1 < ny) s -= (V)kn[c] * x[c + 1];
+    if (iy > 0) s -= (V)kn[c - 1] * x[c - 1];
+    return s;
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double sh[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    __syncthreads();
+    return v;
+}
+
+// r64 = b - L x (FP64); scal[S_RR] += |r|^2, scal[S_BB] += |b|^2
+__global__ void k_resid64(int nx, int ny, const double *d, const double *ke, const double *kn, const double *x,
+                          const double *b, double *r, double *scal) {
+    const int n = nx * ny, rhs = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const double *xr = x + (size_t)rhs * n;
+    double rr = 0, bb = 0;
+    if (c < n) {
+        const double bv = b[(size_t)rhs * n + c];
+        const double v = bv - apply_at(d, ke, kn, xr, nx, ny, c);
+        r[(size_t)rhs * n + c] = v;
+        rr = v * v;
+        bb = bv * bv;
+    }
+    rr = block_sum(rr);
+    bb = block_sum(bb);
+    if (threadIdx.x == 0) {
+        atomicAdd(scal + rhs * 8 + S_RR, rr);
+        atomicAdd(scal + rhs * 8 + S_BB, bb);
+    }
+}
+
+// r32 = r64 / |r64| ; e = 0
+__global__ void k_normalise(int n, const double *r64, float *r32, float *e, double *scal) {
+    const int rhs = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double nr = sqrt(scal[rhs * 8 + S_RR]);
+    const double inv = nr > 0 ? 1.0 / nr : 0.0;
+    r32[(size_t)rhs * n + c] = (float)(r64[(size_t)rhs * n + c] * inv);
+    e[(size_t)rhs * n + c] = 0.f;
+}
+
+// x64 += |r64| * e
+__global__ void k_correct(int n, const float *e, double *x, const double *scal) {
+    const int rhs = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double nr = sqrt(scal[rhs * 8 + S_RR]);
+    x[(size_t)rhs * n + c] += nr * (double)e[(size_t)rhs * n + c];
+}
+
+// Red-black Gauss-Seidel half sweep on one colour (x updated in place).
+__global__ void k_smooth(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
+                         float *x, const float *b, int color) {
+    const int n = nx * ny, rhs = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const int ix = c / ny, iy = c - ix * ny;
+    if (((ix + iy) & 1) != color || fixed[c]) return;
+    float *xr = x + (size_t)rhs * n;
+    const int w = wrapx(ix - 1, nx) * ny + iy, e = wrapx(ix + 1, nx) * ny + iy;
+    float s = b[(size_t)rhs * n + c] + ke[c] * xr[e] + ke[w] * xr[w];
+    if (iy + 1 < ny) s += kn[c] * xr[c + 1];
+    if (iy > 0) s += kn[c - 1] * xr[c - 1];
+    xr[c] = s / d[c];
+}
+
+__global__ void k_zero(size_t n, float *x) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = 0.f;
+}
+
+__global__ void k_resid32(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
+                          const float *x, const float *b, float *r) {
+    const int n = nx * ny, rhs = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const size_t o = (size_t)rhs * n;
+    r[o + c] = fixed[c] ? 0.f : b[o + c] - apply_at(d, ke, kn, x + o, nx, ny, c);
+}
+
+// coarse b = sum of the free fine residuals of the 2x2 aggregate
+__global__ void k_restrict(int fnx, int fny, const uint8_t *ffixed, const float *r, int cnx, int cny, float *b) {
+    const int cn = cnx * cny, fn = fnx * fny, rhs = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cn) return;
+    const int I = c / cny, J = c - I * cny;
+    float s = 0.f;
+    for (int a = 0; a < 2; ++a) {
+        const int i = 2 * I + a;
+        if (i >= fnx) break;
+        for (int q = 0; q < 2; ++q) {
+            const int j = 2 * J + q;
+            if (j >= fny) break;
+            const int f = i * fny + j;
+            if (!ffixed[f]) s += r[(size_t)rhs * fn + f];
+        }
+    }
+    b[(size_t)rhs * cn + c] = s;
+}
+
+__global__ void k_prolong(int fnx, int fny, const uint8_t *ffixed, float *x, int cnx, int cny, const float *xc) {
+    const int fn = fnx * fny, cn = cnx * cny, rhs = blockIdx.y;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= fn || ffixed[f]) return;
+    const int i = f / fny, j = f - i * fny;
+    x[(size_t)rhs * fn + f] += xc[(size_t)rhs * cn + (i >> 1) * cny + (j >> 1)];
+}
+
+// q = L p (FP32, fine level), scal[S_PQ] += p.q
+__global__ void k_matvec_dot(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
+                             const float *p, float *q, double *scal) {
+    const int n = nx * ny, rhs = blockIdx.y;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc = 0;
+    if (c < n) {
+        const size_t o = (size_t)rhs * n;
+        const float v = fixed[c] ? 0.f : apply_at(d, ke, kn, p + o, nx, ny, c);
+        q[o + c] = v;
+        acc = (double)v * (double)p[o + c];
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(scal + rhs * 8 + S_PQ, acc);
+}
+
+// x += a p ; r -= a q with a = rz / pq
+__global__ void k_axpy(int n, const float *p, const float *q, float *x, float *r, const double *scal) {
+    const int rhs = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const double pq = scal[rhs * 8 + S_PQ], rz = scal[rhs * 8 + S_RZ];
+    const float a = (pq > 0 && rz > 0) ? (float)(rz / pq) : 0.f;
+    const size_t o = (size_t)rhs * n + c;
+    x[o] += a * p[o];
+    r[o] -= a * q[o];
+}
+
+// scal[slot] += r.z
+__global__ void k_dot(int n, const float *r, const float *z, double *scal, int slot) {
+    const int rhs = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc = 0;
+    if (c < n) {
+        const size_t o = (size_t)rhs * n + c;
+        acc = (double)r[o] * (double)z[o];
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) atomicAdd(scal + rhs * 8 + slot, acc);
+}
+
+// p = z + b p with b = rz_new / rz (p = z when first)
+__global__ void k_update_p(int n, const float *z, float *p, const double *scal, int first) {
+    const int rhs = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const size_t o = (size_t)rhs * n + c;
+    if (first) { p[o] = z[o]; return; }
+    const double rz = scal[rhs * 8 + S_RZ], rzn = scal[rhs * 8 + S_RZ_NEW];
+    const float beta = rz > 0 ? (float)(rzn / rz) : 0.f;
+    p[o] = z[o] + beta * p[o];
+}
+
+// per-rhs scalar bookkeeping between PCG steps
+__global__ void k_shift_rz(int nrhs, double *scal) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrhs) return;
+    scal[i * 8 + S_RZ] = scal[i * 8 + S_RZ_NEW];
+    scal[i * 8 + S_RZ_NEW] = 0;
+    scal[i * 8 + S_PQ] = 0;
+}
+
+__global__ void k_clear_slots(int nrhs, double *scal, int first, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrhs) return;
+    for (int k = first; k < first + count; ++k) scal[i * 8 + k] = 0;
+}
+
+dim3 grid_for(int n, int nrhs) { return dim3((n + PT - 1) / PT, nrhs); }
+
+// z = M r on the fine level (one symmetric V-cycle); r lives in lev[0].b.
+void vcycle(tb_poisson *ps, int l, int nrhs, cudaStream_t s) {
+    Level &L = ps->lev[l];
+    const size_t tot = (size_t)nrhs * L.n;
+    k_zero<<<(unsigned)((tot + PT - 1) / PT), PT, 0, s>>>(tot, L.x);
+    const dim3 g = grid_for(L.n, nrhs);
+    if (l + 1 == (int)ps->lev.size()) {
+        for (int k = 0; k < ps->coarse_sweeps; ++k) {
+            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
+            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
+        }
+        for (int k = 0; k < ps->coarse_sweeps; ++k) {
+            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
+            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
+        }
+        return;
+    }
+    for (int k = 0; k < ps->pre; ++k) {
+        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
+        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
+    }
+    k_resid32<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, L.r);
+    Level &C = ps->lev[l + 1];
+    k_restrict<<<grid_for(C.n, nrhs), PT, 0, s>>>(L.nx, L.ny, L.fixed, L.r, C.nx, C.ny, C.b);
+    vcycle(ps, l + 1, nrhs, s);
+    k_prolong<<<g, PT, 0, s>>>(L.nx, L.ny, L.fixed, L.x, C.nx, C.ny, C.x);
+    for (int k = 0; k < ps->post; ++k) {
+        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
+        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
+    }
+}
+
+// z = M r : copies r into the level-0 right-hand side, runs the V-cycle, copies x out.
+void precondition(tb_poisson *ps, int nrhs, const float *r, float *z, cudaStream_t s) {
+    Level &L = ps->lev[0];
+    const size_t bytes = (size_t)nrhs * L.n * sizeof(float);
+    cudaMemcpyAsync(L.b, r, bytes, cudaMemcpyDeviceToDevice, s);
+    vcycle(ps, 0, nrhs, s);
+    cudaMemcpyAsync(z, L.x, bytes, cudaMemcpyDeviceToDevice, s);
+}
+
+// Builds the coarse operator of level f into c (host arrays).
+void coarsen(int fnx, int fny, const std::vector<float> &d, const std::vector<float> &ke,
+             const std::vector<float> &kn, const std::vector<uint8_t> &fx, int &cnx, int &cny,
+             std::vector<float> &cd, std::vector<float> &cke, std::vector<float> &ckn, std::vector<uint8_t> &cfx) {
+    cnx = (fnx + 1) / 2;
+    cny = (fny + 1) / 2;
+    const int cn = cnx * cny;
+    std::vector<double> sd(cn, 0.0), se(cn, 0.0), sn(cn, 0.0);
+    std::vector<int> nfree(cn, 0);
+    auto agg = [&](int i, int j) { return (i >> 1) * cny + (j >> 1); };
+    for (int i = 0; i < fnx; ++i) {
+        for (int j = 0; j < fny; ++j) {
+            const int f = i * fny + j;
+            if (fx[f]) continue;
+            const int a = agg(i, j);
+            nfree[a]++;
+            sd[a] += d[f];
+            // east coupling
+            const int ie = i + 1 == fnx ? 0 : i + 1;
+            const int fe = ie * fny + j;
+            if (!fx[fe] && ke[f] != 0.f) {
+                const int b = agg(ie, j);
+                if (b == a) sd[a] -= 2.0 * ke[f];
+                else if (b == (((i >> 1) + 1) == cnx ? 0 : (i >> 1) + 1) * cny + (j >> 1)) se[a] += ke[f];
+            }
+            if (j + 1 < fny && !fx[f + 1] && kn[f] != 0.f) {
+                const int b = agg(i, j + 1);
+                if (b == a) sd[a] -= 2.0 * kn[f];
+                else sn[a] += kn[f];
+            }
+        }
+    }
+    cd.assign(cn, 1.f);
+    cke.assign(cn, 0.f);
+    ckn.assign(cn, 0.f);
+    cfx.assign(cn, 1);
+    for (int a = 0; a < cn; ++a) {
+        if (!nfree[a]) continue;
+        cfx[a] = 0;
+        cd[a] = (float)(0.5 * sd[a]);
+        cke[a] = (float)(0.5 * se[a]);
+        ckn[a] = (float)(0.5 * sn[a]);
+    }
+    // couplings into fixed coarse cells are dropped
+    for (int I = 0; I < cnx; ++I)
+        for (int J = 0; J < cny; ++J) {
+            const int a = I * cny + J;
+            const int e = (I + 1 == cnx ? 0 : I + 1) * cny + J;
+            if (cfx[a] || cfx[e]) cke[a] = 0.f;
+            if (J + 1 >= cny || cfx[a] || cfx[a + 1]) ckn[a] = 0.f;
+        }
+}
+
+template <typename T>
+int upload(tb_ctx *ctx, T **dst, const T *src, size_t n) {
+    TB_CUDA(ctx, cudaMalloc(dst, n * sizeof(T)));
+    if (src) TB_CUDA(ctx, cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    return TB_OK;
+}
+
+}  // namespace
+
+void tb_poisson_free(tb_poisson *ps) {
+    if (!ps) return;
+    for (Level &L : ps->lev) {
+        cudaFree(L.d); cudaFree(L.ke); cudaFree(L.kn); cudaFree(L.fixed);
+        cudaFree(L.x); cudaFree(L.b); cudaFree(L.r);
+    }
+    cudaFree(ps->d64); cudaFree(ps->ke64); cudaFree(ps->kn64); cudaFree(ps->r64);
+    cudaFree(ps->e); cudaFree(ps->pr); cudaFree(ps->pz); cudaFree(ps->pp); cudaFree(ps->pq);
+    cudaFree(ps->scal);
+    delete ps;
+}
+
+extern "C" int tb_poisson_setup(tb_ctx *ctx, const double *h_diag, const double *h_ke, const double *h_kn,
+                                const uint8_t *h_fixed, int max_rhs) {
+    if (!ctx) return TB_ERR_ARG;
+    if (!h_diag || !h_ke || !h_kn || !h_fixed || max_rhs < 1)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_setup: missing operator arrays or max_rhs < 1");
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int nx = ctx->nx, ny = ctx->ny, n = nx * ny;
+    for (int c = 0; c < n; ++c) {
+        if (!h_fixed[c] && !(h_diag[c] > 0))
+            return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_setup: diagonal must be positive on free cells (cell %d)", c);
+        if (h_ke[c] < 0 || h_kn[c] < 0)
+            return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_setup: couplings must be non-negative (cell %d)", c);
+    }
+    if (ctx->poisson) { tb_poisson_free(ctx->poisson); ctx->poisson = nullptr; }
+    tb_poisson *ps = new tb_poisson();
+    ps->max_rhs = max_rhs;
+    // fine level: couplings into fixed cells removed, fixed rows identity
+    std::vector<float> d(n), ke(n), kn(n);
+    std::vector<uint8_t> fx(h_fixed, h_fixed + n);
+    std::vector<double> d64(n), ke64(n), kn64(n);
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            const int c = ix * ny + iy;
+            const int e = (ix + 1 == nx ? 0 : ix + 1) * ny + iy;
+            d64[c] = fx[c] ? 1.0 : h_diag[c];
+            ke64[c] = (fx[c] || fx[e]) ? 0.0 : h_ke[c];
+            kn64[c] = (iy + 1 >= ny || fx[c] || fx[c + 1]) ? 0.0 : h_kn[c];
+            d[c] = (float)d64[c]; ke[c] = (float)ke64[c]; kn[c] = (float)kn64[c];
+        }
+    int rc = TB_OK;
+    if ((rc = upload(ctx, &ps->d64, d64.data(), n)) || (rc = upload(ctx, &ps->ke64, ke64.data(), n)) ||
+        (rc = upload(ctx, &ps->kn64, kn64.data(), n))) {
+        tb_poisson_free(ps);
+        return rc;
+    }
+    int lnx = nx, lny = ny;
+    for (;;) {
+        Level L;
+        L.nx = lnx; L.ny = lny; L.n = lnx * lny;
+        const size_t vec = (size_t)max_rhs * L.n;
+        if ((rc = upload(ctx, &L.d, d.data(), L.n)) || (rc = upload(ctx, &L.ke, ke.data(), L.n)) ||
+            (rc = upload(ctx, &L.kn, kn.data(), L.n)) || (rc = upload(ctx, &L.fixed, fx.data(), L.n)) ||
+            (rc = upload<float>(ctx, &L.x, nullptr, vec)) || (rc = upload<float>(ctx, &L.b, nullptr, vec)) ||
+            (rc = upload<float>(ctx, &L.r, nullptr, vec))) {
+            ps->lev.push_back(L);
+            tb_poisson_free(ps);
+            return rc;
+        }
+        ps->lev.push_back(L);
+        if (L.n <= 64 || lnx <= 2 || lny <= 2 || ps->lev.size() >= 16) break;
+        std::vector<float> cd, cke, ckn;
+        std::vector<uint8_t> cfx;
+        int cnx, cny;
+        coarsen(lnx, lny, d, ke, kn, fx, cnx, cny, cd, cke, ckn, cfx);
+        d.swap(cd); ke.swap(cke); kn.swap(ckn); fx.swap(cfx);
+        lnx = cnx; lny = cny;
+    }
+    const size_t vec = (size_t)max_rhs * n;
+    if ((rc = upload<double>(ctx, &ps->r64, nullptr, vec)) || (rc = upload<float>(ctx, &ps->e, nullptr, vec)) ||
+        (rc = upload<float>(ctx, &ps->pr, nullptr, vec)) || (rc = upload<float>(ctx, &ps->pz, nullptr, vec)) ||
+        (rc = upload<float>(ctx, &ps->pp, nullptr, vec)) || (rc = upload<float>(ctx, &ps->pq, nullptr, vec)) ||
+        (rc = upload<double>(ctx, &ps->scal, nullptr, (size_t)max_rhs * 8))) {
+        tb_poisson_free(ps);
+        return rc;
+    }
+    ctx->poisson = ps;
+    return TB_OK;
+}
+
+extern "C" int tb_poisson_levels(const tb_ctx *ctx) {
+    return (ctx && ctx->poisson) ? (int)ctx->poisson->lev.size() : 0;
+}
+
+extern "C" int tb_poisson_solve(tb_ctx *ctx, int nrhs, const double *d_b, double *d_x, double rtol, int max_outer,
+                                int inner, int *iters, double *h_resid, void *stream) {
+    if (!ctx) return TB_ERR_ARG;
+    tb_poisson *ps = ctx->poisson;
+    if (!ps) return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_solve: call tb_poisson_setup first");
+    if (nrhs < 1 || nrhs > ps->max_rhs || !d_b || !d_x || !(rtol > 0) || max_outer < 1 || inner < 1)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_solve: invalid arguments (nrhs=%d, max_rhs=%d)", nrhs,
+                       ps->max_rhs);
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const Level &F = ps->lev[0];
+    const int n = F.n;
+    const dim3 g = grid_for(n, nrhs);
+    const unsigned sb = (unsigned)((nrhs + PT - 1) / PT);
+    std::vector<double> sc((size_t)nrhs * 8);
+    int outer = 0;
+    double worst = 0;
+    for (;;) {
+        k_clear_slots<<<sb, PT, 0, s>>>(nrhs, ps->scal, 0, 8);
+        k_resid64<<<g, PT, 0, s>>>(F.nx, F.ny, ps->d64, ps->ke64, ps->kn64, d_x, d_b, ps->r64, ps->scal);
+        TB_CUDA(ctx, cudaMemcpyAsync(sc.data(), ps->scal, sc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        TB_CUDA(ctx, cudaStreamSynchronize(s));
+        worst = 0;
+        bool done = true;
+        for (int k = 0; k < nrhs; ++k) {
+            const double rr = sqrt(sc[k * 8 + S_RR]), bb = sqrt(sc[k * 8 + S_BB]);
+            const double rel = bb > 0 ? rr / bb : rr;
+            if (rel > worst) worst = rel;
+            if (!(rel <= rtol)) done = false;
+        }
+        if (done || outer >= max_outer) break;
+        ++outer;
+        // FP32 PCG on L e = r / |r|
+        k_normalise<<<g, PT, 0, s>>>(n, ps->r64, ps->pr, ps->e, ps->scal);
+        for (int it = 0; it < inner; ++it) {
+            precondition(ps, nrhs, ps->pr, ps->pz, s);
+            k_dot<<<g, PT, 0, s>>>(n, ps->pr, ps->pz, ps->scal, S_RZ_NEW);
+            k_update_p<<<g, PT, 0, s>>>(n, ps->pz, ps->pp, ps->scal, it == 0);
+            k_shift_rz<<<sb, PT, 0, s>>>(nrhs, ps->scal);
+            k_matvec_dot<<<g, PT, 0, s>>>(F.nx, F.ny, F.d, F.ke, F.kn, F.fixed, ps->pp, ps->pq, ps->scal);
+            k_axpy<<<g, PT, 0, s>>>(n, ps->pp, ps->pq, ps->e, ps->pr, ps->scal);
+        }
+        k_correct<<<g, PT, 0, s>>>(n, ps->e, d_x, ps->scal);
+        TB_CUDA(ctx, cudaGetLastError());
+    }
+    if (iters) *iters = outer;
+    if (h_resid) *h_resid = worst;
+    if (!(worst <= rtol))
+        return tb_fail(ctx, TB_ERR_CONVERGENCE, "Poisson solve reached %d refinement steps at relative residual %.3e",
+                       outer, worst);
+    return TB_OK;
+}

@@ -1,0 +1,264 @@
+// Per-batch charge and field update on the device (everything after the trace).
+//
+// Restates the reference batch loop body (trench_charging_2d.py:1239-1285):
+//   deposit     drho = (cnt_i - cnt_e) q / dx^2, zero on conductors      (:1240-1243)
+//   leakage     Qs_new = M (rho_s dx^2 + dt G phi_ext)                    (:1246-1256)
+//   conductor   driven: rho = 0 on it; floating: semi-implicit step       (:1257-1266, :815-830)
+//   potential   phi = solve(-rho/eps0) + external                         (:1268)
+//   field       E = -grad phi over vacuum neighbours                      (:1269, :429-454)
+//   history     bottom flux ratios, escapes, lost, leak, probe potentials (:1272-1280)
+//
+// Charge only ever sits on surface cells (every absorbing cell is a solid cell
+// next to vacuum), so the state is the surface vector rho_s (m entries, FP64)
+// and the potential is phi = external + G rho_s, with G the surface Green's
+// operator (built once with the multigrid solver).  Both products are
+// bandwidth-bound GEMVs, one warp per row.  The field kernel writes the FP64
+// field (reference layout) and the packed FP32 tracer field in one pass.
+//
+// Compiled with -fmad=false so the field and deposit arithmetic rounds like
+// the reference's NumPy expressions.
+#include <math.h>
+
+#include "tb_internal.cuh"
+
+namespace {
+
+constexpr int ONE_BLOCK = 1024;
+
+enum { H_RATIO_I = 0, H_RATIO_E = 1, H_ESC_E = 2, H_LOST = 3, H_LEAK = 4, H_STEPS = 5, H_PROBE0 = 6 };
+
+__device__ double block_reduce(double v, double *sh) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// numpy.logaddexp
+__device__ double logaddexp(double x, double y) {
+    if (x == y) return x + 0.693147180559945309417232121458176568;
+    const double t = x - y;
+    if (t > 0) return x + log1p(exp(-t));
+    if (t <= 0) return y + log1p(exp(t));
+    return t;  // NaN
+}
+
+// Semi-implicit floating-conductor potential step (trench_charging_2d.py:815-830).
+__device__ double conductor_step(double n_i, double n_e, double q, double C, double Te, double drift) {
+    const double x_i = q * n_i / C + drift, x_e = q * n_e / C;
+    if (n_e == 0) return x_i;
+    const double k = x_i / Te;
+    const double frac = k != 0 ? -expm1(-k) / k : 1.0;
+    return -Te * logaddexp(-k, log(x_e / Te * frac));
+}
+
+// K1: deposit counts on the surface vector, leakage input, tallies.
+__global__ void __launch_bounds__(ONE_BLOCK) k_deposit(const tb_step_desc d, int ncell, double *tally, int *err) {
+    __shared__ double sh[32];
+    if (threadIdx.x == 0) *d.d_batch += 1;
+    const double dx2 = d.dx * d.dx;
+    double ni = 0, ne = 0, bi = 0, be = 0, hi = 0, he = 0, reg = 0;
+    for (int s = threadIdx.x; s < d.m; s += blockDim.x) {
+        const int c = d.d_surf[s];
+        const int ci = d.d_counts[c], ce = d.d_counts[ncell + c];
+        const uint8_t f = d.d_sflag[s];
+        const double rp = d.d_rho_s[s];
+        d.d_rho_prev[s] = rp;
+        double drho = ((double)(ci - ce) * d.q_macro) / dx2;
+        if (f & TB_SFLAG_COND) drho = 0.0;
+        const double r = rp + drho;
+        d.d_rho_s[s] = r;
+        const double qs = r * dx2;
+        d.d_work[s] = d.d_leak_h ? qs + d.d_leak_h[s] : qs;
+        if (f & TB_SFLAG_COND) { ni += ci; ne += ce; }
+        if (f & TB_SFLAG_BOTTOM) { bi += ci; be += ce; }
+        if (f & TB_SFLAG_REGION) reg += qs;
+        hi += ci;
+        he += ce;
+    }
+    ni = block_reduce(ni, sh); ne = block_reduce(ne, sh);
+    bi = block_reduce(bi, sh); be = block_reduce(be, sh);
+    hi = block_reduce(hi, sh); he = block_reduce(he, sh);
+    reg = block_reduce(reg, sh);
+    if (threadIdx.x == 0) {
+        tally[0] = ni; tally[1] = ne; tally[2] = bi; tally[3] = be; tally[4] = reg;
+        // every absorbed particle must have landed on a surface cell
+        if ((long long)hi != d.d_totals[4] || (long long)he != d.d_totals[5])
+            atomicCAS(err, TB_DERR_NONE, TB_DERR_OFF_SURFACE);
+    }
+}
+
+// y = A x with A row-major (rows, cols); one warp per row, FP64 accumulation.
+template <typename T>
+__global__ void k_gemv(int rows, int cols, const T *A, const double *x, double *y, const double *y0,
+                       const int32_t *scatter) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= rows) return;
+    const T *a = A + (size_t)warp * cols;
+    double acc = 0.0;
+    for (int c = lane; c < cols; c += 32) acc += (double)a[c] * x[c];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+        if (scatter) {
+            const int cell = scatter[warp];
+            y[cell] = y0[cell] + acc;
+        } else {
+            y[warp] = acc;
+        }
+    }
+}
+
+// K3: leakage result, conductor step, history scalars.
+__global__ void __launch_bounds__(ONE_BLOCK) k_finish(const tb_step_desc d, const double *tally) {
+    __shared__ double sh[32];
+    const double dx2 = d.dx * d.dx;
+    const bool leak = d.d_leak_M != nullptr;
+    double reg_new = 0, drift = 0;
+    for (int s = threadIdx.x; s < d.m; s += blockDim.x) {
+        const uint8_t f = d.d_sflag[s];
+        double r = d.d_rho_s[s];
+        if (leak) {
+            const double qn = d.d_work[d.m + s];
+            r = qn / dx2;
+            if (f & TB_SFLAG_REGION) reg_new += qn;
+        }
+        if (d.driven && (f & TB_SFLAG_COND)) r = 0.0;
+        d.d_rho_s[s] = r;
+        if (d.floating) drift += (r - d.d_rho_prev[s]) * d.d_g_s[s];
+    }
+    reg_new = block_reduce(reg_new, sh);
+    drift = block_reduce(drift, sh);
+    if (threadIdx.x == 0) {
+        const int row = *d.d_batch;
+        double leak_ratio = 0.0;
+        if (leak) leak_ratio = (tally[4] - reg_new) / d.dt_batch / d.leak_norm;
+        if (d.floating && d.c_slot >= 0) {
+            drift = drift * dx2;
+            const double dV = conductor_step(tally[0], tally[1], d.q_macro, d.C_cond, d.Te, drift);
+            d.d_rho_s[d.c_slot] += d.C_cond * (dV - drift) / dx2;
+        }
+        if (row >= 0 && row < d.max_batches) {
+            double *h = d.d_hist + (size_t)row * d.hist_cols;
+            h[H_RATIO_I] = tally[2] / d.bottom_norm;
+            h[H_RATIO_E] = tally[3] / d.bottom_norm;
+            h[H_ESC_E] = (double)d.d_totals[1] / d.n_per_batch;
+            h[H_LOST] = (double)d.d_totals[2] / (2.0 * d.n_per_batch);
+            h[H_LEAK] = leak_ratio;
+            h[H_STEPS] = (double)d.d_totals[3];
+        }
+    }
+}
+
+// K5: E = -grad phi over vacuum neighbours (trench_charging_2d.py:429-454), the
+// packed FP32 tracer field, the per-face wall barrier and the probe history.
+__global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac, double scale_e, double scale_phi,
+                        tb_fcell *out, float4 *bar, int padded) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = nx * ny;
+    if (c == 0) {
+        const int row = *d.d_batch;
+        if (row >= 0 && row < d.max_batches)
+            for (int k = 0; k < d.n_probes; ++k)
+                d.d_hist[(size_t)row * d.hist_cols + H_PROBE0 + k] = d.d_phi[d.d_probes[k]];
+    }
+    if (c >= padded) return;
+    if (c >= n) { out[c] = tb_fcell{0.f, 0.f}; return; }
+    const int ix = c / ny, iy = c - ix * ny;
+    const int w = (ix == 0 ? nx - 1 : ix - 1) * ny + iy, e = (ix == nx - 1 ? 0 : ix + 1) * ny + iy;
+    const double *phi = d.d_phi;
+    const double pc = phi[c];
+    const double dx = d.dx;
+    // x: neighbours west (m) and east (pl)
+    double gx = 0.0;
+    {
+        const bool vm = vac[w], vp = vac[e];
+        const double m = phi[w], pl = phi[e];
+        if (vm && vp) gx = (pl - m) / (2 * dx);
+        else if (vp) gx = (pl - pc) / dx;
+        else if (vm) gx = (pc - m) / dx;
+    }
+    double gy = 0.0;
+    {
+        const bool vm = iy > 0 ? vac[c - 1] : false;
+        const bool vp = iy < ny - 1 ? vac[c + 1] : true;
+        const double m = iy > 0 ? phi[c - 1] : 2 * d.v_sub - pc;
+        const double pl = iy < ny - 1 ? phi[c + 1] : (d.top_dirichlet ? 2 * d.v_top - pc : pc);
+        if (vm && vp) gy = (pl - m) / (2 * dx);
+        else if (vp) gy = (pl - pc) / dx;
+        else if (vm) gy = (pc - m) / dx;
+    }
+    const double ex = -gx, ey = -gy;
+    if (d.d_ex) { d.d_ex[c] = ex; d.d_ey[c] = ey; }
+    const int v = vac[c] ? 1 : 0;
+    const float fx = (float)(ex * (double)v * scale_e);
+    const float fy = (float)(ey * (double)v * scale_e);
+    uint32_t bx = __float_as_uint(fx);
+    bx = v ? (bx | 1u) : (bx & ~1u);
+    out[c] = tb_fcell{__uint_as_float(bx), fy};
+    float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!v && d.d_wface) {
+        const double f = d.d_wface[c];
+        b.x = (float)(f * (pc - phi[w]) * scale_phi);
+        b.y = (float)(f * (pc - phi[e]) * scale_phi);
+        b.z = iy > 0 ? (float)(f * (pc - phi[c - 1]) * scale_phi) : 0.f;
+        b.w = iy < ny - 1 ? (float)(f * (pc - phi[c + 1]) * scale_phi) : 0.f;
+    }
+    bar[c] = b;
+}
+
+}  // namespace
+
+extern "C" int tb_step_charge(tb_ctx *ctx, const tb_step_desc *d, void *stream) {
+    if (!ctx || !d) return TB_ERR_ARG;
+    if (d->m < 1 || !d->d_surf || !d->d_sflag || !d->d_rho_s || !d->d_rho_prev || !d->d_work || !d->d_counts ||
+        !d->d_totals || !d->d_batch || !d->d_hist || d->hist_cols < 6 || !(d->dx > 0) || !(d->bottom_norm > 0) ||
+        !(d->n_per_batch > 0))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_step_charge: incomplete step descriptor");
+    if (d->floating && (!d->d_g_s || !(d->C_cond > 0)))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_step_charge: floating conductor needs g_s and C_cond");
+    if (d->d_leak_M && !(d->dt_batch > 0 && d->leak_norm > 0))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_step_charge: leakage needs dt_batch and leak_norm");
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    double *tally = reinterpret_cast<double *>(ctx->d_queue + 2);  // 5 doubles of context scratch
+    k_deposit<<<1, ONE_BLOCK, 0, s>>>(*d, ctx->nx * ctx->ny, tally, ctx->d_err);
+    if (d->d_leak_M) {
+        const int threads = 256, wpb = threads / 32;
+        k_gemv<double><<<(d->m + wpb - 1) / wpb, threads, 0, s>>>(d->m, d->m, d->d_leak_M, d->d_work,
+                                                                  d->d_work + d->m, nullptr, nullptr);
+    }
+    k_finish<<<1, ONE_BLOCK, 0, s>>>(*d, tally);
+    TB_CUDA(ctx, cudaGetLastError());
+    return TB_OK;
+}
+
+extern "C" int tb_step_potential(tb_ctx *ctx, const tb_step_desc *d, void *stream) {
+    if (!ctx || !d) return TB_ERR_ARG;
+    if (d->n_rows < 1 || !d->d_rows || (!d->d_green && !d->d_green64) || !d->d_ext || !d->d_phi ||
+        !(d->vscale > 0))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_step_potential: incomplete step descriptor");
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = (cudaStream_t)stream;
+    const int threads = 256, wpb = threads / 32;
+    const int blocks = (d->n_rows + wpb - 1) / wpb;
+    if (d->d_green)
+        k_gemv<float><<<blocks, threads, 0, s>>>(d->n_rows, d->m, d->d_green, d->d_rho_s, d->d_phi, d->d_ext,
+                                                 d->d_rows);
+    else
+        k_gemv<double><<<blocks, threads, 0, s>>>(d->n_rows, d->m, d->d_green64, d->d_rho_s, d->d_phi, d->d_ext,
+                                                  d->d_rows);
+    const int cells = ctx->nx * ctx->ny, padded = (cells + 1) & ~1;
+    const double scale_e = ctx->dx / (d->vscale * d->vscale), scale_phi = 1.0 / (d->vscale * d->vscale);
+    k_field<<<(padded + 255) / 256, 256, 0, s>>>(*d, ctx->nx, ctx->ny, ctx->d_vac, scale_e, scale_phi, ctx->d_field,
+                                                ctx->d_barrier, padded);
+    TB_CUDA(ctx, cudaGetLastError());
+    ctx->vscale = d->vscale;
+    ctx->fields_ready = 1;
+    return TB_OK;
+}

@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
     float ox = 0.f, oy = 0.f, vx = 0.f, vy = 0.f, qm = 0.f;
     bool open = true;
     unsigned long long my_steps = 0;
-    unsigned my_esc_i = 0, my_esc_e = 0, my_lost = 0;
+    unsigned my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
 
     for (;;) {
         const unsigned need = __ballot_sync(FULL, pid < 0);
@@ -244,6 +244,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
                 atomicAdd(a.d_counts + (size_t)spc * cells + dcell, 1);
             }
             if (a.d_hit) a.d_hit[pid] = dcell;
+            if (spc == 0) ++my_hit_i; else ++my_hit_e;
             done = 1;
         } else if (escaped) {
             if (spc == 0) ++my_esc_i; else ++my_esc_e;
@@ -271,6 +272,8 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         my_esc_i += __shfl_down_sync(FULL, my_esc_i, o);
         my_esc_e += __shfl_down_sync(FULL, my_esc_e, o);
         my_lost += __shfl_down_sync(FULL, my_lost, o);
+        my_hit_i += __shfl_down_sync(FULL, my_hit_i, o);
+        my_hit_e += __shfl_down_sync(FULL, my_hit_e, o);
     }
     if (lane == 0) {
         unsigned long long *t = reinterpret_cast<unsigned long long *>(a.d_totals);
@@ -278,6 +281,8 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         if (my_esc_e) atomicAdd(t + 1, (unsigned long long)my_esc_e);
         if (my_lost) atomicAdd(t + 2, (unsigned long long)my_lost);
         if (my_steps) atomicAdd(t + 3, my_steps);
+        if (my_hit_i) atomicAdd(t + 4, (unsigned long long)my_hit_i);
+        if (my_hit_e) atomicAdd(t + 5, (unsigned long long)my_hit_e);
     }
 }
 
@@ -330,6 +335,16 @@ int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const
     return TB_OK;
 }
 
+// Raises the dynamic shared-memory limit of the FP32 tracer to the device maximum.
+// Called from tb_create, so launches (also inside a CUDA graph capture) make no
+// attribute calls; the attribute is per function and device, always this value.
+int tb_configure_trace_f32(tb_ctx *ctx) {
+    const int limit = ctx->max_smem - 1024;
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+    ctx->smem_attr_bytes = limit;
+    return TB_OK;
+}
+
 int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     K32 k;
     k.a = *a;
@@ -345,15 +360,11 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     const int cells = ctx->nx * ctx->ny;
     k.bytes = ((cells + 1) & ~1) * (int)sizeof(tb_fcell);
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
-    int max_smem = 0;
-    TB_CUDA(ctx, cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
-    const bool smem = k.bytes + 1024 <= max_smem;
+    const bool smem = k.bytes <= ctx->smem_attr_bytes;
     long long want = (a->n + F32_THREADS - 1) / F32_THREADS;
     int blocks = (int)(want < ctx->num_sms ? want : ctx->num_sms);
     if (blocks < 1) blocks = 1;
     if (smem) {
-        TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          k.bytes));
         trace_f32_kernel<true><<<blocks, F32_THREADS, k.bytes, s>>>(k);
     } else {
         trace_f32_kernel<false><<<blocks, F32_THREADS, 0, s>>>(k);

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
     double x = 0, y = 0, vx = 0, vy = 0, qm = 0, clock = 0, elapsed = 0, xp = 0, yp = 0;
     int steps = 0, stop_at = 0, spc = 0, slot = -1, plen = 0;
     bool open = true;
-    unsigned long long my_steps = 0, my_esc_i = 0, my_esc_e = 0, my_lost = 0;
+    unsigned long long my_steps = 0, my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
 
     for (;;) {
         // Refill empty lanes from the global queue (one atomic per warp).
@@ -272,6 +272,7 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
                 atomicAdd(a.d_counts + (size_t)spc * cells + cell, 1);
             }
             if (a.d_hit) a.d_hit[pid] = (int32_t)cell;
+            if (spc == 0) ++my_hit_i; else ++my_hit_e;
             done = 1;
         } else if (escaped) {
             if (spc == 0) ++my_esc_i; else ++my_esc_e;
@@ -303,6 +304,8 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
         my_esc_i += __shfl_down_sync(FULL, my_esc_i, o);
         my_esc_e += __shfl_down_sync(FULL, my_esc_e, o);
         my_lost += __shfl_down_sync(FULL, my_lost, o);
+        my_hit_i += __shfl_down_sync(FULL, my_hit_i, o);
+        my_hit_e += __shfl_down_sync(FULL, my_hit_e, o);
     }
     if (lane == 0) {
         unsigned long long *t = reinterpret_cast<unsigned long long *>(a.d_totals);
@@ -310,6 +313,8 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
         if (my_esc_e) atomicAdd(t + 1, my_esc_e);
         if (my_lost) atomicAdd(t + 2, my_lost);
         if (my_steps) atomicAdd(t + 3, my_steps);
+        if (my_hit_i) atomicAdd(t + 4, (unsigned long long)my_hit_i);
+        if (my_hit_e) atomicAdd(t + 5, (unsigned long long)my_hit_e);
     }
 }
 

@@ -1,0 +1,208 @@
+"""Poisson operator, boundary potentials and the multigrid solver on the device.
+
+Host-side assembly (once per case) restates the reference's operator and
+boundary terms; the solve runs on the GPU through ``tb_poisson_setup`` /
+``tb_poisson_solve`` (multigrid-preconditioned CG, FP32 V-cycles, FP64
+refinement).  ``FieldSolver.solve`` is a drop-in for the reference's
+``fields["solve"]`` (trench_charging_2d.py:297-309, 378-392): it takes the
+right-hand side b of A phi = b (flat, or column-stacked), and returns phi with
+the same conductor semantics (floating conductor as one unknown, driven
+conductor held at zero).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi
+from .params import EPS0, FIELD_MODES, SIDE_BCS
+
+
+def poisson_matrix_arrays(eps, cond, p):
+    """Diagonal and east/north face coefficients of div(eps grad) (trench_charging_2d.py:252-294).
+
+    Returns (diag, ce, cn) with A phi = diag*phi + ce*phi_E + cw*phi_W + cn*phi_N + cs*phi_S,
+    cw = roll(ce, 1), cs[:, 1:] = cn[:, :-1]; cn[:, -1] = 0.
+    """
+    nx, ny = eps.shape
+    dx2 = p.dx ** 2
+
+    def face(a, b, ca, cb):
+        h = np.where(ca, 2.0 * b, np.where(cb, 2.0 * a, 2.0 * a * b / (a + b)))
+        return np.where(ca & cb, 0.0, h)
+
+    ce = face(eps, np.roll(eps, -1, axis=0), cond, np.roll(cond, -1, axis=0)) / dx2
+    top_ox = p.floor_t + p.trench_d
+    if p.side_bc != "periodic":
+        ce[-1, :top_ox] = 0.0
+    cw = np.roll(ce, 1, axis=0)
+    c_int = face(eps[:, :-1], eps[:, 1:], cond[:, :-1], cond[:, 1:]) / dx2
+    cn = np.zeros((nx, ny)); cn[:, :-1] = c_int
+    cs = np.zeros((nx, ny)); cs[:, 1:] = c_int
+    diag_n, diag_s = cn.copy(), cs.copy()
+    diag_s[:, 0] += 2.0 * eps[:, 0] / dx2
+    if p.top_bc == "dirichlet":
+        diag_n[:, -1] += 2.0 * eps[:, -1] / dx2
+    diag = -(ce + cw + diag_n + diag_s)
+    if p.side_bc != "periodic":
+        diag[0, :top_ox] -= 2.0 * eps[0, :top_ox] / dx2
+        diag[-1, :top_ox] -= 2.0 * eps[-1, :top_ox] / dx2
+    return diag, ce, cn
+
+
+def apply_matrix(diag, ce, cn, phi):
+    """A @ phi for the arrays of poisson_matrix_arrays (phi shaped (nx, ny))."""
+    out = diag * phi + ce * np.roll(phi, -1, axis=0) + np.roll(ce, 1, axis=0) * np.roll(phi, 1, axis=0)
+    out[:, :-1] += cn[:, :-1] * phi[:, 1:]
+    out[:, 1:] += cn[:, :-1] * phi[:, :-1]
+    return out
+
+
+def boundary_rhs(p, eps, volts, fixed_sides=True):
+    """Right-hand side of the boundary potentials (trench_charging_2d.py:323-337)."""
+    rhs = np.zeros_like(eps)
+    rhs[:, 0] -= 2.0 * eps[:, 0] / p.dx ** 2 * volts["substrate"]
+    if p.top_bc == "dirichlet":
+        rhs[:, -1] -= 2.0 * eps[:, -1] / p.dx ** 2 * volts["top"]
+    top_ox = p.floor_t + p.trench_d
+    if p.side_bc == "pillar":
+        yfrac = (np.arange(top_ox) + 0.5) / top_ox
+        vl = vr = volts["substrate"] + (volts["mask"] - volts["substrate"]) * yfrac
+    else:
+        vl, vr = (p.left_voltage, p.right_voltage) if fixed_sides else (0.0, 0.0)
+    if p.side_bc != "periodic":
+        rhs[0, :top_ox] -= 2.0 * eps[0, :top_ox] / p.dx ** 2 * vl
+        rhs[-1, :top_ox] -= 2.0 * eps[-1, :top_ox] / p.dx ** 2 * vr
+    return rhs
+
+
+def circuit_voltages(c, phase):
+    """Periodic interpolation of the circuit potentials (trench_charging_2d.py:312-320)."""
+    t = np.asarray(c["t"])
+    period = (t[1] - t[0]) * t.size
+    at = (phase % 360.0) / 360.0 * period
+    values = {k: float(np.interp(at, np.append(t, period), np.append(c[k], c[k][0])))
+              for k in ("uw", "um", "up", "V1")}
+    return dict(substrate=values["uw"] - values["up"], mask=values["um"] - values["up"],
+                top=0.0, sheath=values["V1"])
+
+
+def field_voltages(p, mask, circuit=None):
+    """Validation and electrode voltages of setup_fields (trench_charging_2d.py:342-374)."""
+    if p.field_mode not in FIELD_MODES or p.side_bc not in SIDE_BCS:
+        raise ValueError("invalid field_mode or side_bc")
+    if p.top_bc not in ("dirichlet", "neumann"):
+        raise ValueError("top_bc must be dirichlet or neumann")
+    numeric = (p.rf_phase, p.substrate_voltage, p.mask_voltage, p.top_voltage, p.left_voltage, p.right_voltage)
+    if not np.isfinite(numeric).all():
+        raise ValueError("voltages and RF phase must be finite")
+    driven = p.field_mode != "floating"
+    if driven and mask.any() and p.mask_type != "conductor":
+        raise ValueError("a mask voltage needs mask_type=conductor")
+    if p.side_bc == "pillar" and not driven:
+        raise ValueError("the pillar boundary needs field_mode fixed / circuit / circuit_rf")
+    if p.field_mode in ("circuit", "circuit_rf"):
+        if p.bias != "rf" or circuit is None or p.top_bc != "dirichlet":
+            raise ValueError("circuit field modes need bias=rf and top_bc=dirichlet")
+    if p.field_mode == "circuit":
+        return circuit_voltages(circuit, p.rf_phase)
+    if p.field_mode == "circuit_rf":
+        wave = np.column_stack((circuit["uw"] - circuit["up"], circuit["um"] - circuit["up"]))
+        mean = wave.mean(axis=0)
+        return dict(substrate=float(mean[0]), mask=float(mean[1]), top=0.0, sheath=float(np.mean(circuit["V1"])))
+    return dict(substrate=p.substrate_voltage, mask=p.mask_voltage, top=p.top_voltage)
+
+
+class FieldSolver:
+    """Multigrid solve of A phi = b on the device with the reference's conductor semantics.
+
+    mode "none": plain solve; "driven": conductor cells held at 0; "floating":
+    all conductor cells share one potential set by their total charge (the
+    reduced system E^T A E of trench_charging_2d.py:297-309), done here by
+    superposition: phi = phi0 + V psi with phi0 solved with the conductor at 0,
+    psi the unit-conductor-potential response and V from the conductor row.
+    """
+
+    RTOL = 1e-13
+
+    def __init__(self, ctx, p, eps, cond, driven, max_rhs=64):
+        self.ctx = ctx
+        self.nx, self.ny = eps.shape
+        self.n = self.nx * self.ny
+        self.dev = torch.device("cuda", ctx.device)
+        self.dx2 = p.dx ** 2
+        self.diag, self.ce, self.cn = poisson_matrix_arrays(eps, cond, p)
+        self.cond = np.asarray(cond, bool)
+        self.mode = "none" if not self.cond.any() else ("driven" if driven else "floating")
+        # SPD form L = -dx^2 A
+        d = -self.diag * self.dx2
+        ke = self.ce * self.dx2
+        kn = self.cn * self.dx2
+        fixed = self.cond.astype(np.uint8) if self.mode != "none" else np.zeros((self.nx, self.ny), np.uint8)
+        self.max_rhs = int(max_rhs)
+        L = _capi.lib()
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        ctx.check(L.tb_poisson_setup(ctx.handle, f(d).ctypes.data_as(ctypes.c_void_p),
+                                     f(ke).ctypes.data_as(ctypes.c_void_p), f(kn).ctypes.data_as(ctypes.c_void_p),
+                                     np.ascontiguousarray(fixed).ctypes.data_as(ctypes.c_void_p), self.max_rhs))
+        self.levels = L.tb_poisson_levels(ctx.handle)
+        self.cond_t = torch.from_numpy(self.cond.ravel()).to(self.dev)
+        self.last_iters = 0
+        self.last_resid = 0.0
+        if self.mode == "floating":
+            # coupling of free cells to the conductor, w_f = sum over conductor neighbours of k_fc
+            c = self.cond
+            w = np.zeros((self.nx, self.ny))
+            east_c, west_c = np.roll(c, -1, axis=0), np.roll(c, 1, axis=0)
+            w += np.where(~c & east_c, ke, 0.0)
+            w += np.where(~c & west_c, np.roll(ke, 1, axis=0), 0.0)
+            w[:, :-1] += np.where(~c[:, :-1] & c[:, 1:], kn[:, :-1], 0.0)
+            w[:, 1:] += np.where(~c[:, 1:] & c[:, :-1], kn[:, :-1], 0.0)
+            self.w = torch.from_numpy(w.ravel()).to(self.dev)
+            psi = self._solve_spd(self.w[None, :].clone())[0]
+            self.psi = psi
+            self.D = float(d[c].sum()) - float(torch.dot(self.w, psi))
+
+    def _solve_spd(self, bp, x0=None):
+        """L x = bp for rows of bp (k, n) on the device (fixed cells must be zero)."""
+        L = _capi.lib()
+        k = bp.shape[0]
+        out = torch.zeros_like(bp) if x0 is None else x0.clone()
+        stream = torch.cuda.current_stream(self.dev)
+        iters, resid = ctypes.c_int(), ctypes.c_double()
+        for s in range(0, k, self.max_rhs):
+            e = min(k, s + self.max_rhs)
+            b = bp[s:e].contiguous()
+            x = out[s:e].contiguous()
+            self.ctx.check(L.tb_poisson_solve(self.ctx.handle, e - s, ctypes.c_void_p(b.data_ptr()),
+                                              ctypes.c_void_p(x.data_ptr()), self.RTOL, 40, 12,
+                                              ctypes.byref(iters), ctypes.byref(resid),
+                                              ctypes.c_void_p(stream.cuda_stream)))
+            out[s:e] = x
+            self.last_iters = max(self.last_iters, iters.value)
+            self.last_resid = max(self.last_resid, resid.value)
+        return out
+
+    def solve_rows(self, b):
+        """A phi = b for the rows of b (k, n) given as a device tensor; returns (k, n)."""
+        bp = -self.dx2 * b
+        if self.mode == "none":
+            return self._solve_spd(bp)
+        bc = (bp * self.cond_t).sum(dim=1)                 # conductor part of the right-hand side
+        bp = torch.where(self.cond_t[None, :], torch.zeros_like(bp), bp)
+        phi0 = self._solve_spd(bp)
+        if self.mode == "driven":
+            return phi0
+        V = (bc + phi0 @ self.w) / self.D
+        phi = phi0 + V[:, None] * self.psi[None, :]
+        return torch.where(self.cond_t[None, :], V[:, None].expand_as(phi), phi)
+
+    def solve(self, b):
+        """Drop-in for fields["solve"]: b is (n,) or (n, k) host or device; returns the same layout."""
+        host = not isinstance(b, torch.Tensor)
+        bt = torch.as_tensor(np.asarray(b, dtype=np.float64) if host else b, device=self.dev, dtype=torch.float64)
+        one = bt.dim() == 1
+        rows = bt[None, :] if one else bt.T.contiguous()
+        x = self.solve_rows(rows)
+        x = x[0] if one else x.T
+        return x.cpu().numpy() if host else x

@@ -1,0 +1,339 @@
+"""ChargingCase: the reference batch loop with every per-batch stage on the GPU.
+
+Mirrors trench_charging_2d.run (trench_charging_2d.py:1045-1369) for the hot
+path: per batch the particles are traced, deposited, leaked, the conductor is
+stepped, the potential and field are recomputed and the history is recorded,
+all on the device (kernels of libtrench_b200.so) with no host synchronisation.
+The host supplies injected particles (``load``), or the caller captures one
+batch in a CUDA graph (``capture``) and replays it.
+
+Setup (once per case) builds the multigrid hierarchy, the external potential,
+the floating-conductor response, the surface Green's operator G (potential on
+the vacuum and surface cells per unit charge density on each surface cell) and
+the implicit leakage operator M = inv(I - dt G_leak P) (trench_charging_2d.py:768-803)
+from multigrid solves on the GPU.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi, geometry
+from .fields import FieldSolver, apply_matrix, boundary_rhs, field_voltages
+from .inject import inject
+from .params import E_CHARGE, EPS0, WALL_MODELS, is_tapered
+from .tracer import DEFAULT_VSCALE, Context, _ptr
+
+HIST_SCALARS = ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost", "leak", "particle_steps")
+
+
+class ChargingCase:
+    def __init__(self, p, device=0, precision="f32", green="f32", circuit=None, max_batches=None,
+                 capacity=None, vscale=DEFAULT_VSCALE, max_rhs=64):
+        if precision not in _capi.PRECISION:
+            raise ValueError(f"precision must be one of {tuple(_capi.PRECISION)}")
+        if green not in ("f32", "f64"):
+            raise ValueError("green must be f32 or f64")
+        if p.wall_model not in WALL_MODELS:
+            raise ValueError(f"wall_model must be one of {WALL_MODELS}: {p.wall_model!r}")
+        if p.field_mode == "circuit_rf":
+            raise ValueError("field_mode circuit_rf is traced by B200Tracer(rf=...); the device batch loop "
+                             "covers floating / fixed / circuit")
+        if not (0 < p.cfl <= 1) or p.max_steps < 1:
+            raise ValueError("CUDA tracing needs 0 < cfl <= 1 and max_steps >= 1")
+        if not torch.cuda.is_available():
+            raise RuntimeError("no CUDA device is visible (the B200 backend has no CPU path)")
+        self.p = p
+        self.precision = precision
+        self.vscale = float(vscale)
+        self.dev = torch.device("cuda", int(device))
+        solid, mask, i0, i1 = geometry.build_geometry(p)
+        self.solid, self.mask, self.i0, self.i1 = solid, mask, i0, i1
+        self.vac = vac = ~solid
+        nx, ny = solid.shape
+        self.nx, self.ny, self.n = nx, ny, nx * ny
+        dev = self.dev
+        with torch.cuda.device(dev):
+            self.ctx = Context(vac, int(device), p.dx)
+            self.volts = volts = field_voltages(p, mask, circuit)
+            cond = mask if p.mask_type == "conductor" else np.zeros_like(mask)
+            eps = geometry.permittivity(solid, mask, p)
+            driven = p.field_mode != "floating"
+            self.cond, self.eps = cond, eps
+            self.solver = solver = FieldSolver(self.ctx, p, eps, cond, driven, max_rhs=max_rhs)
+            # external potential (trench_charging_2d.py:378-394)
+            if driven and cond.any():
+                phi_cond = cond.astype(float) * volts["mask"]
+                mask_rhs = -apply_matrix(solver.diag, solver.ce, solver.cn, phi_cond)
+            else:
+                phi_cond = np.zeros((nx, ny))
+                mask_rhs = np.zeros((nx, ny))
+            rhs = boundary_rhs(p, eps, volts)
+            self.external = (solver.solve((rhs + mask_rhs).ravel()) + phi_cond.ravel()).reshape(nx, ny)
+            self.floating = bool(cond.any() and not driven)
+            self.driven = driven
+            wface = np.where(cond, 1.0, eps / (1.0 + eps))
+            self.wface = wface
+            # surface cells, Green's rows, probes
+            sx, sy = np.nonzero(geometry.surface_cells(solid))
+            S = sx * ny + sy
+            self.S = S
+            m = self.m = len(S)
+            self.probes = geometry.probe_cells(solid, p, bool(cond.any()))
+            probe_flat = np.array([ix * ny + iy for ix, iy in self.probes.values()], dtype=np.int64)
+            rows = np.union1d(np.union1d(np.flatnonzero(vac.ravel()), S), probe_flat)
+            self.rows = rows
+            self._build_green(rows, green)
+            # leakage (trench_charging_2d.py:768-803)
+            self.leak_M = self.leak_h = None
+            b0, b1 = geometry.opening_span(solid, p.floor_t)
+            e0, e1 = geometry.opening_span(solid, p.floor_t + p.trench_d + p.mask_t - 1)
+            self.b0, self.b1, self.e0, self.e1 = b0, b1, e0, e1
+            cut = p.floor_t + p.trench_d // 2
+            region = geometry.inner_surface_cells(solid, p)[sx, sy] & (sy < cut)
+            if p.sigma_s > 0:
+                Gl = self._leak_graph(sx, sy)
+                self.leak_G = Gl
+                P = self.P
+                Mt = torch.linalg.inv(torch.eye(m, dtype=torch.float64, device=dev)
+                                      - p.dt_batch * (torch.from_numpy(Gl).to(dev) @ P))
+                self.leak_M = Mt.contiguous()
+                if np.any(self.external):
+                    h = p.dt_batch * (Gl @ self.external.ravel()[S])
+                    self.leak_h = torch.from_numpy(h).to(dev)
+            # floating conductor (trench_charging_2d.py:1087-1090, 807-812)
+            self.g_s = None
+            self.C_cond, self.c_slot = 0.0, -1
+            if self.floating:
+                b = np.zeros(self.n)
+                b[np.flatnonzero(cond)[0]] = -1.0 / (p.dx ** 2 * EPS0)
+                g = solver.solve(b)
+                self.g_cond = g.reshape(nx, ny)
+                self.C_cond = 1.0 / g[np.flatnonzero(cond)[0]]
+                c_cell = np.flatnonzero(geometry.surface_cells(solid) & cond)[0]
+                self.c_slot = int(np.flatnonzero(S == c_cell)[0])
+                self.g_s = torch.from_numpy(g[S]).to(dev)
+            # flags
+            sflag = np.zeros(m, np.uint8)
+            sflag[cond.ravel()[S]] |= _capi.SFLAG_COND
+            sflag[region] |= _capi.SFLAG_REGION
+            sflag[(sy == p.floor_t - 1) & (sx >= b0) & (sx < b1)] |= _capi.SFLAG_BOTTOM
+            self.q_macro = E_CHARGE * (p.flux * (nx * p.dx) * p.dt_batch / p.n_per_batch)
+            # device state
+            self.max_batches = int(max_batches or max(p.n_batches, 1))
+            self.hist_cols = len(HIST_SCALARS) + len(self.probes)
+            cap = int(capacity or 2 * p.n_per_batch)
+            self.capacity = cap
+            f64 = torch.float64
+            self.t_surf = torch.from_numpy(S.astype(np.int32)).to(dev)
+            self.t_sflag = torch.from_numpy(sflag).to(dev)
+            self.rho_s = torch.zeros(m, dtype=f64, device=dev)
+            self.rho_prev = torch.zeros(m, dtype=f64, device=dev)
+            self.work = torch.zeros(2 * m, dtype=f64, device=dev)
+            self.t_rows = torch.from_numpy(rows.astype(np.int32)).to(dev)
+            self.t_ext = torch.from_numpy(self.external.ravel().copy()).to(dev)
+            self.phi = self.t_ext.clone()
+            self.ex = torch.zeros(self.n, dtype=f64, device=dev)
+            self.ey = torch.zeros(self.n, dtype=f64, device=dev)
+            self.t_wface = torch.from_numpy(wface.ravel().copy()).to(dev)
+            self.hist = torch.zeros((self.max_batches, self.hist_cols), dtype=f64, device=dev)
+            self.t_probes = torch.from_numpy(probe_flat.astype(np.int32)).to(dev)
+            self.batch = torch.full((1,), -1, dtype=torch.int32, device=dev)
+            self.counts = torch.zeros((2, self.n), dtype=torch.int32, device=dev)
+            self.totals = torch.zeros(8, dtype=torch.int64, device=dev)
+            self.X = [torch.zeros(cap, dtype=f64, device=dev) for _ in range(5)]  # x, y, vx, vy, qm
+            self.SPC = torch.zeros(cap, dtype=torch.int8, device=dev)
+            self.status = torch.full((cap,), 3, dtype=torch.int8, device=dev)
+            self.steps = torch.zeros(cap, dtype=torch.int32, device=dev)
+            self.n_loaded = 0
+            self._desc = self._make_desc(m, sflag)
+            self._args = _capi.TraceArgs()
+            self._graph = None
+            self.trace_events = None   # optional (start, end) CUDA events around the tracer launch
+            # initial field (trench_charging_2d.py:1198)
+            self._potential()
+
+    # ---- setup helpers -----------------------------------------------------------
+    def _build_green(self, rows, green):
+        """G[r, j] = potential at rows[r] per unit charge density on surface cell j."""
+        p, dev, S, m = self.p, self.dev, self.S, self.m
+        dtype = torch.float32 if green == "f32" else torch.float64
+        G = torch.empty((len(rows), m), dtype=dtype, device=dev)
+        P = torch.empty((m, m), dtype=torch.float64, device=dev)
+        t_rows = torch.from_numpy(rows).to(dev)
+        t_S = torch.from_numpy(S).to(dev)
+        chunk = self.solver.max_rhs
+        for s in range(0, m, chunk):
+            e = min(m, s + chunk)
+            b = torch.zeros((e - s, self.n), dtype=torch.float64, device=dev)
+            b[torch.arange(e - s, device=dev), t_S[s:e]] = -1.0 / EPS0
+            x = self.solver.solve_rows(b)
+            G[:, s:e] = x[:, t_rows].T.to(dtype)
+            P[:, s:e] = x[:, t_S].T / p.dx ** 2   # per unit charge (1 C/m) on a dx^2 cell
+        self.G = G.contiguous()
+        self.P = P
+        self.green = green
+
+    def _leak_graph(self, sx, sy):
+        """Conductance graph of the surface cells (trench_charging_2d.py:778-792)."""
+        p, nx, ny, m = self.p, self.nx, self.ny, self.m
+        smap = -np.ones((nx, ny), dtype=np.int64)
+        smap[sx, sy] = np.arange(m)
+        g = p.sigma_s / p.dx
+        G = np.zeros((m, m))
+        for a, b in ((smap, np.roll(smap, -1, axis=0)), (smap[:, :-1], smap[:, 1:])):
+            sel = (a >= 0) & (b >= 0)
+            a, b = a[sel], b[sel]
+            np.add.at(G, (a, b), g)
+            np.add.at(G, (b, a), g)
+            np.add.at(G, (a, a), -g)
+            np.add.at(G, (b, b), -g)
+        return G
+
+    def _make_desc(self, m, sflag):
+        p = self.p
+        d = _capi.StepDesc()
+        d.m = m
+        d.d_surf, d.d_sflag = _ptr(self.t_surf), _ptr(self.t_sflag)
+        d.d_rho_s, d.d_rho_prev, d.d_work = _ptr(self.rho_s), _ptr(self.rho_prev), _ptr(self.work)
+        d.d_leak_M, d.d_leak_h, d.d_g_s = _ptr(self.leak_M), _ptr(self.leak_h), _ptr(self.g_s)
+        d.c_slot = self.c_slot
+        d.floating, d.driven = int(self.floating), int(self.driven)
+        d.q_macro, d.dx, d.C_cond, d.Te = self.q_macro, float(p.dx), float(self.C_cond), float(p.electron_temp_eV)
+        d.dt_batch = float(p.dt_batch)
+        d.leak_norm = float(E_CHARGE * p.flux * (self.e1 - self.e0) * p.dx)
+        d.bottom_norm = float(p.n_per_batch * ((self.b1 - self.b0) / self.nx))
+        d.n_per_batch = float(p.n_per_batch)
+        d.n_rows = len(self.rows)
+        d.d_rows = _ptr(self.t_rows)
+        d.d_green = _ptr(self.G) if self.green == "f32" else None
+        d.d_green64 = _ptr(self.G) if self.green == "f64" else None
+        d.d_ext, d.d_phi = _ptr(self.t_ext), _ptr(self.phi)
+        d.d_ex, d.d_ey = _ptr(self.ex), _ptr(self.ey)
+        d.d_wface = _ptr(self.t_wface) if p.wall_model == "barrier" else None
+        d.v_sub, d.v_top = float(p.substrate_voltage), float(self.volts["top"])
+        d.top_dirichlet = int(p.top_bc == "dirichlet")
+        d.vscale = self.vscale
+        d.d_hist = _ptr(self.hist)
+        d.hist_cols, d.max_batches = self.hist_cols, self.max_batches
+        d.n_probes = len(self.probes)
+        d.d_probes, d.d_batch = _ptr(self.t_probes), _ptr(self.batch)
+        d.d_counts, d.d_totals = _ptr(self.counts), _ptr(self.totals)
+        return d
+
+    def _stream(self):
+        return ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+
+    def _potential(self):
+        self.ctx.check(_capi.lib().tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), self._stream()))
+
+    # ---- per batch -----------------------------------------------------------------
+    def load(self, x, y, vx, vy, qm, spc, non_blocking=False):
+        """Copy one batch of injected particles into the device buffers."""
+        n = len(x)
+        if n > self.capacity:
+            raise ValueError(f"{n} particles exceed the case capacity {self.capacity}")
+        if any(len(v) != n for v in (y, vx, vy, qm, spc)):
+            raise ValueError("particle arrays differ in length")
+        for dst, src in zip(self.X, (x, y, vx, vy, qm)):
+            t = src if isinstance(src, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(src, np.float64))
+            dst[:n].copy_(t, non_blocking=non_blocking)
+        t = spc if isinstance(spc, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(spc, np.int8))
+        self.SPC[:n].copy_(t, non_blocking=non_blocking)
+        self.n_loaded = n
+
+    def step(self, n=None):
+        """One charging batch on the current stream (trace, deposit, leakage, conductor, potential, field)."""
+        L = _capi.lib()
+        n = self.n_loaded if n is None else n
+        p = self.p
+        s = self._stream()
+        self.status[:n].fill_(3)
+        self.steps[:n].zero_()
+        self.counts.zero_()
+        self.totals.zero_()
+        a = self._args
+        a.n = n
+        a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in self.X)
+        a.d_spc = _ptr(self.SPC)
+        a.d_ex, a.d_ey = _ptr(self.ex), _ptr(self.ey)
+        bar = p.wall_model == "barrier"
+        a.d_phi, a.d_wface = (_ptr(self.phi), _ptr(self.t_wface)) if bar else (None, None)
+        a.max_steps = a.step_budget = int(p.max_steps)
+        a.cfl = float(p.cfl)
+        a.tapered = int(is_tapered(p))
+        a.d_counts, a.d_totals = _ptr(self.counts), _ptr(self.totals)
+        a.d_status, a.d_steps = _ptr(self.status), _ptr(self.steps)
+        a.d_hit = None
+        a.write_state = 0
+        ev = getattr(self, "trace_events", None)
+        if ev is not None:
+            ev[0].record()
+        if n:
+            self.ctx.check(L.tb_trace(self.ctx.handle, ctypes.byref(a), _capi.PRECISION[self.precision], s))
+        if ev is not None:
+            ev[1].record()
+        self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
+        self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
+
+    def capture(self, n=None):
+        """Capture one batch (for n particles already in the buffers) as a CUDA graph."""
+        n = self.n_loaded if n is None else n
+        side = torch.cuda.Stream(self.dev)
+        side.wait_stream(torch.cuda.current_stream(self.dev))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(g, stream=side):
+                self.step(n)
+        torch.cuda.current_stream(self.dev).wait_stream(side)
+        self._graph = g
+        return g
+
+    def replay(self):
+        self._graph.replay()
+
+    def check(self):
+        """Synchronise and raise if a kernel recorded a failed check."""
+        self.ctx.check(_capi.lib().tb_check(self.ctx.handle, self._stream()))
+
+    # ---- results -------------------------------------------------------------------
+    def batches_done(self):
+        return int(self.batch.item()) + 1
+
+    def history(self):
+        nb = min(self.batches_done(), self.max_batches)
+        h = self.hist[:nb].cpu().numpy()
+        out = {k: h[:, i].copy() for i, k in enumerate(HIST_SCALARS)}
+        for j, k in enumerate(self.probes):
+            out[k] = h[:, len(HIST_SCALARS) + j].copy()
+        out["t"] = np.arange(1, nb + 1) * self.p.dt_batch
+        return out
+
+    def rho(self):
+        r = np.zeros(self.n)
+        r[self.S] = self.rho_s.cpu().numpy()
+        return r.reshape(self.nx, self.ny)
+
+    def full_potential(self):
+        """phi on every cell: solve(-rho/eps0) + external (trench_charging_2d.py:1268)."""
+        rho = self.rho()
+        return (self.solver.solve((-rho / EPS0).ravel()) + self.external.ravel()).reshape(self.nx, self.ny)
+
+    def fields(self):
+        return (self.ex.cpu().numpy().reshape(self.nx, self.ny), self.ey.cpu().numpy().reshape(self.nx, self.ny))
+
+    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None):
+        """The reference batch loop (trench_charging_2d.py:1225-1285) with host injection."""
+        p = self.p
+        n_batches = p.n_batches if n_batches is None else n_batches
+        rng = np.random.default_rng(p.seed) if rng is None else rng
+        with torch.cuda.device(self.dev):
+            for b in range(n_batches):
+                self.load(*inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity))
+                self.step()
+                if log is not None and ((b + 1) % 10 == 0 or b == 0):
+                    log(f"[{b + 1}/{n_batches}]")
+            self.check()
+        ex, ey = self.fields()
+        return dict(rho_raw=self.rho(), mean_phi=self.full_potential(), Ex=ex, Ey=ey, hist=self.history(),
+                    solid=self.solid, mask=self.mask, probes=self.probes, backend_used="b200")

@@ -155,7 +155,7 @@ class B200Tracer:
         if barrier is not None:
             PHI, WF = self._dev(barrier[0], f64), self._dev(barrier[1], f64)
         counts = torch.zeros((2, nx, ny), dtype=torch.int32, device=dev)
-        totals = torch.zeros(4, dtype=torch.int64, device=dev)
+        totals = torch.zeros(8, dtype=torch.int64, device=dev)
         status = torch.full((n,), 3, dtype=torch.int8, device=dev)
         hit = torch.full((n,), -1, dtype=torch.int32, device=dev)
         steps = torch.zeros(n, dtype=torch.int32, device=dev)
