@@ -242,6 +242,7 @@ def run_b200(args, p):
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     trace_ms = []
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
     wall0 = time.perf_counter()
     for k in range(args.steps):
         src = dev_pool[(args.warmup + k) % pool_n]
@@ -258,6 +259,7 @@ def run_b200(args, p):
         trace_ms.append(t0e.elapsed_time(t1e))
     torch.cuda.synchronize()
     wall = time.perf_counter() - wall0
+    torch.cuda.nvtx.range_pop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
     if world > 1:
@@ -321,7 +323,7 @@ def run_b200(args, p):
             "kernel": "trace_f32_kernel", "trace_ms_per_launch": float(np.mean(trace_ms)),
             "particle_steps_per_launch": mean_steps,
             "particle_steps_per_s": float(np.mean([s / (t / 1000.0) for s, t in zip(steps_per_batch, trace_ms)]))}
-    cpu = cpu_baseline(p, 1 << 15, seconds_budget=float(os.environ.get("TB_CPU_SECONDS", "15")))
+    cpu = cpu_baseline(p, 1 << 15, seconds_budget=args.cpu_seconds)
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -357,10 +359,12 @@ def main():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--particles", type=int, default=1 << 19, help="particles per species per batch")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample duration")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    p = workload()
+    p = workload(args.particles)
     if args.impl == "reference":
         return run_reference(args, p)
     return run_b200(args, p)

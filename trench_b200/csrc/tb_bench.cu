@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(1024, 1) k_smem_read(int words, int iters, flo
 extern "C" int tb_bench_smem(tb_ctx *ctx, double *gbs) {
     if (!ctx || !gbs) return TB_ERR_ARG;
     TB_CUDA(ctx, cudaSetDevice(ctx->device));
-    const int words = 8192;  // 64 KiB of float2
+    const int words = 4096;  // 32 KiB of float2 (below the default dynamic limit)
     const int threads = 1024, iters = 1 << 14;
     const int blocks = ctx->num_sms;
     float *sink = nullptr;
@@ -38,8 +38,11 @@ extern "C" int tb_bench_smem(tb_ctx *ctx, double *gbs) {
     TB_CUDA(ctx, cudaEventCreate(&a));
     TB_CUDA(ctx, cudaEventCreate(&b));
     k_smem_read<<<blocks, threads, words * sizeof(float2)>>>(words, iters, sink);  // warm-up
+    TB_CUDA(ctx, cudaGetLastError());
+    TB_CUDA(ctx, cudaDeviceSynchronize());
     TB_CUDA(ctx, cudaEventRecord(a));
     k_smem_read<<<blocks, threads, words * sizeof(float2)>>>(words, iters, sink);
+    TB_CUDA(ctx, cudaGetLastError());
     TB_CUDA(ctx, cudaEventRecord(b));
     TB_CUDA(ctx, cudaEventSynchronize(b));
     float ms = 0;

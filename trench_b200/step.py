@@ -28,7 +28,7 @@ HIST_SCALARS = ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost", "leak", "pa
 
 
 class ChargingCase:
-    def __init__(self, p, device=0, precision="f32", green="f32", circuit=None, max_batches=None,
+    def __init__(self, p, device=0, precision="f32", green="f64", circuit=None, max_batches=None,
                  capacity=None, vscale=DEFAULT_VSCALE, max_rhs=64):
         if precision not in _capi.PRECISION:
             raise ValueError(f"precision must be one of {tuple(_capi.PRECISION)}")
