@@ -170,6 +170,26 @@ int tb_step_charge(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
  * tb_set_fields) and probe history. */
 int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
 
+/* ---- No-allocation FP32 tracer ---------------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc -- a
+ * host application whose memory pool owns all device memory, or a caller that must
+ * not let cudaMalloc/cudaFree synchronise the device -- this entry point allocates
+ * nothing and needs no context: the tracer's scratch (packed FP32 field, wall
+ * barrier, work-queue counter, check flag) lives in a static device array of about
+ * 1.5 MiB that every GPU loading the library holds until the process exits.  It
+ * traces like tb_trace with TB_PRECISION_F32 on the current device; the caller
+ * passes the device vacuum mask d_vac (nx*ny bytes, 1 = vacuum), the FP64 fields
+ * in args->d_ex/d_ey (and d_phi/d_wface for the barrier model) and every input and
+ * output array.  Grids above TB_NOALLOC_MAX_CELLS cells are rejected (TB_ERR_ARG).
+ * args->d_totals[6] receives the device check flag (0 = every bound held).  The
+ * first call on a device looks up the array's device address and configures the
+ * kernel; make that first call before any stream capture.  All calls share the
+ * one array, so calls that overlap on the GPU (other streams, other host threads)
+ * race: serialise them.  Errors are read with tb_last_error(NULL). */
+#define TB_NOALLOC_MAX_CELLS 65536
+int tb_trace_f32_noalloc(int nx, int ny, double dx, const uint8_t *d_vac, const tb_trace_args *args,
+                         double vscale, void *stream);
+
 /* Measured shared-memory load bandwidth of the context's GPU (GB/s, all SMs, 8-byte
  * loads like the FP32 tracer's gathers).  A benchmark helper; synchronises the device. */
 int tb_bench_smem(tb_ctx *ctx, double *gbs);

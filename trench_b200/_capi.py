@@ -91,6 +91,8 @@ SIGNATURES = {
     "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
+    "tb_trace_f32_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dbl, _vp, ctypes.POINTER(TraceArgs),
+                                            _dbl, _vp]),
 }
 
 _lib = None

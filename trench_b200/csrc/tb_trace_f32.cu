@@ -372,3 +372,100 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     TB_CUDA(ctx, cudaGetLastError());
     return TB_OK;
 }
+
+// ---------------------------------------------------------------------------------
+// No-allocation variant of the FP32 tracer.
+//
+// Some callers cannot call cudaMalloc: a host application that hands every byte of
+// device memory to its own pool at start-up, or a caller on a latency-critical
+// path where cudaMalloc/cudaFree may synchronise the whole device.  For them
+// tb_trace_f32_noalloc keeps the tracer's scratch -- the packed FP32 field, the
+// per-face wall barrier, the work-queue counter and the check flag -- in the
+// file-scope array below instead of a context.  Every GPU that loads this
+// library holds the array (about 1.5 MiB) until the process exits.
+
+namespace {
+
+constexpr size_t NOALLOC_FIELD_BYTES = (size_t)TB_NOALLOC_MAX_CELLS * sizeof(tb_fcell);
+constexpr size_t NOALLOC_BARRIER_BYTES = (size_t)TB_NOALLOC_MAX_CELLS * sizeof(float4);
+constexpr size_t NOALLOC_COUNTER_BYTES = 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_FIELD_BYTES + NOALLOC_BARRIER_BYTES + NOALLOC_COUNTER_BYTES;
+
+// Host code must not pass this name to a kernel: on the host it is a stand-in,
+// not a device address.  The per-device address comes from cudaGetSymbolAddress.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+struct NoallocDevice {
+    unsigned char *base = nullptr;  // device address of g_noalloc_scratch on this device
+    int num_sms = 0;
+    int max_smem = 0;
+    int smem_attr_bytes = 0;
+};
+NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+
+}  // namespace
+
+extern "C" int tb_trace_f32_noalloc(int nx, int ny, double dx, const uint8_t *d_vac, const tb_trace_args *a,
+                                    double vscale, void *stream) {
+    if (nx < 1 || ny < 1 || !(dx > 0) || !d_vac || !a || !(vscale > 0))
+        return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: invalid grid, mask or arguments");
+    if ((long long)nx * ny > TB_NOALLOC_MAX_CELLS)
+        return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: grid of %lld cells exceeds the %d-cell maximum",
+                       (long long)nx * ny, TB_NOALLOC_MAX_CELLS);
+    if (a->n < 0 || !(a->cfl > 0 && a->cfl <= 1) || a->max_steps < 1 || a->step_budget < 1)
+        return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: needs n >= 0, 0 < cfl <= 1, max_steps >= 1");
+    if (a->n > 0 && (!a->d_x || !a->d_y || !a->d_vx || !a->d_vy || !a->d_qm || !a->d_spc || !a->d_ex ||
+                     !a->d_ey || !a->d_counts || !a->d_totals || !a->d_status || !a->d_steps))
+        return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: a required array is missing");
+    if ((a->d_phi == nullptr) != (a->d_wface == nullptr))
+        return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: phi and wface must be given together");
+    if (a->n_phase > 0 || a->record)
+        return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: RF clock and record are not supported");
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return tb_fail(nullptr, TB_ERR_DEVICE, "tb_trace_f32_noalloc: no usable current device");
+    NoallocDevice &d = g_noalloc_dev[dev];
+    tb_ctx tmp;  // a view of the static scratch; owns nothing and is never released
+    tmp.device = dev;
+    if (!d.base) {
+        // set-up, once per device with that device current
+        void *ptr = nullptr;
+        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+        cudaDeviceProp prop;
+        e = cudaGetDeviceProperties(&prop, dev);
+        if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaGetDeviceProperties");
+        tmp.max_smem = (int)prop.sharedMemPerBlockOptin;
+        if (tb_configure_trace_f32(&tmp) != TB_OK) return tb_fail(nullptr, TB_ERR_CUDA, "%s", tmp.err);
+        d.num_sms = prop.multiProcessorCount;
+        d.max_smem = tmp.max_smem;
+        d.smem_attr_bytes = tmp.smem_attr_bytes;
+        d.base = static_cast<unsigned char *>(ptr);
+    }
+    tmp.nx = nx;
+    tmp.ny = ny;
+    tmp.dx = dx;
+    tmp.num_sms = d.num_sms;
+    tmp.max_smem = d.max_smem;
+    tmp.smem_attr_bytes = d.smem_attr_bytes;
+    tmp.d_vac = const_cast<uint8_t *>(d_vac);
+    tmp.d_field = reinterpret_cast<tb_fcell *>(d.base);
+    tmp.d_barrier = reinterpret_cast<float4 *>(d.base + NOALLOC_FIELD_BYTES);
+    tmp.d_queue = reinterpret_cast<unsigned long long *>(d.base + NOALLOC_FIELD_BYTES + NOALLOC_BARRIER_BYTES);
+    tmp.d_err = reinterpret_cast<int *>(tmp.d_queue + 8);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a->n == 0) return TB_OK;
+    // the array keeps the previous call's contents: clear the counters that must start at zero
+    e = cudaMemsetAsync(tmp.d_queue, 0, NOALLOC_COUNTER_BYTES, s);
+    if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaMemsetAsync(scratch counters)");
+    if (tb_launch_pack_fields(&tmp, a->d_ex, a->d_ey, a->d_phi, a->d_wface, vscale, s) != TB_OK ||
+        tb_launch_trace_f32(&tmp, a, s) != TB_OK)
+        return tb_fail(nullptr, TB_ERR_CUDA, "%s", tmp.err);
+    // the device check flag goes to totals[6] (0 = every bound held)
+    e = cudaMemsetAsync(a->d_totals + 6, 0, sizeof(int64_t), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a->d_totals + 6, tmp.d_err, sizeof(int), cudaMemcpyDeviceToDevice, s);
+    if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "copy of the check flag");
+    return TB_OK;
+}
