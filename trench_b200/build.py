@@ -21,7 +21,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROO
 UNITS = {
     "tb_capi.cu": [],
     "tb_trace_f64.cu": ["-fmad=false"],
-    "tb_trace_f32.cu": [],
+    "tb_trace_f32.cu": ["-prec-div=false", "-prec-sqrt=false", "-ftz=true"],
     "tb_poisson.cu": [],
     "tb_step.cu": ["-fmad=false"],
     "tb_bench.cu": [],

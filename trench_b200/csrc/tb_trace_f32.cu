@@ -1,5 +1,8 @@
 // FP32 tracer (precision TB_PRECISION_F32): the throughput path.
 //
+// Compiled with -prec-div=false -prec-sqrt=false -ftz=true: divisions and square
+// roots are the hardware approximations (max 2 ulp), denormals flush to zero (the
+// vacuum flag stored in the low bit of a zero field is such a denormal).
 // Design (B200-first):
 //  * Position = integer cell + FP32 offset in [0,1) cell units, so the cell
 //    index, periodic wrap and floor are exact integer operations and the offset
@@ -30,6 +33,7 @@ struct K32 {
     int nx, ny;
     double dx, vscale;
     float inv_v;                    // the reference's "+1 m/s" in velocity units
+    double inv_dx, inv_v64;         // metres -> cells, m/s -> velocity units
     const tb_fcell *field;          // packed field (global)
     const float4 *barrier;          // per-cell face barrier, potential / vscale^2
     unsigned long long *queue;
@@ -37,8 +41,9 @@ struct K32 {
     int bytes;                      // packed field bytes (multiple of 16)
 };
 
+// 1.0f for a vacuum cell, 0.0f for a solid one, with integer operations only
 __device__ __forceinline__ float vac_of(const tb_fcell &c) {
-    return (float)(__float_as_uint(c.ex) & 1u);
+    return __uint_as_float((__float_as_uint(c.ex) & 1u) ? 0x3f800000u : 0u);
 }
 
 template <bool SMEM>
@@ -125,59 +130,60 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
     unsigned my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
 
     for (;;) {
+        // One ballot per iteration: refill empty lanes from the global queue (one
+        // atomic per warp) or leave once the queue is drained and every lane is empty.
         const unsigned need = __ballot_sync(FULL, pid < 0);
-        if (need != 0u && open) {
-            const int leader = __ffs(need) - 1;
-            const int cnt = __popc(need);
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(k.queue, (unsigned long long)cnt);
-            base = __shfl_sync(FULL, base, leader);
-            if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
-            if (pid < 0) {
-                const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
-                if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
-                    pid = (long long)idx;
-                    const double xc = a.d_x[pid] / k.dx, yc = a.d_y[pid] / k.dx;
-                    ix = (int)xc;
-                    if (ix > nx - 1) ix = nx - 1;
-                    if (ix < 0) ix = 0;
-                    iy = (int)floor(yc);
-                    ox = (float)(xc - (double)ix);
-                    oy = (float)(yc - (double)iy);
-                    ox = ox >= 1.f ? ONE_BELOW : (ox < 0.f ? 0.f : ox);
-                    oy = oy >= 1.f ? ONE_BELOW : (oy < 0.f ? 0.f : oy);
-                    vx = (float)(a.d_vx[pid] / k.vscale);
-                    vy = (float)(a.d_vy[pid] / k.vscale);
-                    qm = (float)a.d_qm[pid];
-                    spc = a.d_spc[pid];
-                    steps = a.d_steps[pid];
-                    stop_at = min(a.max_steps, steps + a.step_budget);
+        if (need != 0u) {
+            if (!open) {
+                if (need == FULL) break;
+            } else {
+                const int leader = __ffs(need) - 1;
+                const int cnt = __popc(need);
+                unsigned long long base = 0;
+                if (lane == leader) base = atomicAdd(k.queue, (unsigned long long)cnt);
+                base = __shfl_sync(FULL, base, leader);
+                if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
+                if (pid < 0) {
+                    const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
+                    if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
+                        pid = (long long)idx;
+                        const double xc = a.d_x[pid] * k.inv_dx, yc = a.d_y[pid] * k.inv_dx;
+                        ix = min(max((int)xc, 0), nx - 1);
+                        iy = (int)floor(yc);
+                        ox = fminf(fmaxf((float)(xc - (double)ix), 0.f), ONE_BELOW);
+                        oy = fminf(fmaxf((float)(yc - (double)iy), 0.f), ONE_BELOW);
+                        vx = (float)(a.d_vx[pid] * k.inv_v64);
+                        vy = (float)(a.d_vy[pid] * k.inv_v64);
+                        qm = (float)a.d_qm[pid];
+                        spc = a.d_spc[pid];
+                        steps = a.d_steps[pid];
+                        stop_at = min(a.max_steps, steps + a.step_budget);
+                    }
                 }
             }
         }
-        if (__ballot_sync(FULL, pid >= 0) == 0u) {
-            if (!open) break;
-            continue;
-        }
         if (pid < 0) continue;
 
-        // ---- field at the current position ----
-        int i0, i1, j0, j1;
-        float tx, ty;
-        if (ox >= 0.5f) { tx = ox - 0.5f; i0 = ix; i1 = ix + 1 == nx ? 0 : ix + 1; }
-        else { tx = ox + 0.5f; i0 = ix == 0 ? nx - 1 : ix - 1; i1 = ix; }
-        const int iyc = iy < 0 ? 0 : (iy > ny - 1 ? ny - 1 : iy);
-        if (oy >= 0.5f) { ty = oy - 0.5f; j0 = iyc; j1 = iy + 1 > ny - 1 ? ny - 1 : (iy + 1 < 0 ? 0 : iy + 1); }
-        else { ty = oy + 0.5f; j0 = iy - 1 < 0 ? 0 : (iy - 1 > ny - 1 ? ny - 1 : iy - 1); j1 = iyc; }
-        const tb_fcell c00 = F.at(i0 * ny + j0), c10 = F.at(i1 * ny + j0);
-        const tb_fcell c01 = F.at(i0 * ny + j1), c11 = F.at(i1 * ny + j1);
-        const float w00 = (1.f - tx) * (1.f - ty), w10 = tx * (1.f - ty);
-        const float w01 = (1.f - tx) * ty, w11 = tx * ty;
+        // ---- field at the current position: vacuum-weighted bilinear (branch-free) ----
+        const bool hx = ox >= 0.5f, hy = oy >= 0.5f;
+        const float tx = hx ? ox - 0.5f : ox + 0.5f;
+        const float ty = hy ? oy - 0.5f : oy + 0.5f;
+        int i0 = hx ? ix : ix - 1;
+        i0 = i0 < 0 ? nx - 1 : i0;
+        int i1 = hx ? ix + 1 : ix;
+        i1 = i1 >= nx ? 0 : i1;
+        const int j0 = min(max(hy ? iy : iy - 1, 0), ny - 1);
+        const int j1 = min(max(hy ? iy + 1 : iy, 0), ny - 1);
+        const int r0 = i0 * ny, r1 = i1 * ny;
+        const tb_fcell c00 = F.at(r0 + j0), c10 = F.at(r1 + j0);
+        const tb_fcell c01 = F.at(r0 + j1), c11 = F.at(r1 + j1);
+        const float ux = 1.f - tx, uy = 1.f - ty;
+        const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
         const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
         const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
         const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
-        const float inv_sw = 1.f / fmaxf(sw, 1e-12f);
-        const float ax = qm * (sex * inv_sw), ay = qm * (sey * inv_sw);
+        const float qs = qm / fmaxf(sw, 1e-12f);
+        const float ax = qs * sex, ay = qs * sey;
 
         // ---- CFL step and trapezoid update ----
         const float speed = sqrtf(vx * vx + vy * vy);
@@ -185,56 +191,62 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         const float dt = cfl / (speed + sqrtf(2.f * acc) + k.inv_v);
         const float vxn = vx + ax * dt, vyn = vy + ay * dt;
         const float sx = 0.5f * (vx + vxn) * dt, sy = 0.5f * (vy + vyn) * dt;
-        const int ix0 = ix, iy0 = iy;
-        const float ox0 = ox, oy0 = oy;
-        ox += sx;
-        oy += sy;
-        int dix = 0, diy = 0;
-        if (ox >= 1.f) { ox -= 1.f; dix = 1; }
-        else if (ox < 0.f) { ox += 1.f; dix = -1; if (ox >= 1.f) ox = ONE_BELOW; }
-        if (oy >= 1.f) { oy -= 1.f; diy = 1; }
-        else if (oy < 0.f) { oy += 1.f; diy = -1; if (oy >= 1.f) oy = ONE_BELOW; }
-        ix = ix0 + dix;
-        ix = ix < 0 ? ix + nx : (ix >= nx ? ix - nx : ix);
-        iy = iy0 + diy;
-        vx = vxn; vy = vyn;
+        float nox = ox + sx, noy = oy + sy;
+        const int dix = (nox >= 1.f) ? 1 : ((nox < 0.f) ? -1 : 0);
+        const int diy = (noy >= 1.f) ? 1 : ((noy < 0.f) ? -1 : 0);
+        nox = dix > 0 ? nox - 1.f : (dix < 0 ? nox + 1.f : nox);
+        noy = diy > 0 ? noy - 1.f : (diy < 0 ? noy + 1.f : noy);
+        nox = fminf(nox, ONE_BELOW);
+        noy = fminf(noy, ONE_BELOW);
+        int nix = ix + dix;
+        nix = nix < 0 ? nx - 1 : (nix >= nx ? 0 : nix);
+        const int niy = iy + diy;
         ++steps;
         ++my_steps;
+        const bool escaped = niy >= ny;
+        const int iyn = min(max(niy, 0), ny - 1);
+        const int y0c = min(max(iy, 0), ny - 1);
+        const int diy_e = iyn - y0c;   // row change with both rows clipped like the reference
+        const bool hit_end = !escaped && !F.vac(nix * ny + iyn);
+        const bool corner = tapered && !escaped && !hit_end && dix != 0 && diy_e != 0;
 
-        const bool escaped = iy >= ny;
-        const int iyn = iy < 0 ? 0 : iy;  // iy < ny here unless escaped
-        bool hit = !escaped && !F.vac(ix * ny + iyn);
-        int dcell = ix * ny + iyn;
-        if (!escaped && (hit ? first_face : (tapered && dix != 0))) {
+        if (!(hit_end || corner || escaped || steps >= stop_at)) {
+            ix = nix; iy = niy; ox = nox; oy = noy; vx = vxn; vy = vyn;
+            continue;
+        }
+
+        // ---- rare path: wall contact, escape, or step cap ----
+        bool hit = hit_end;
+        int dcell = nix * ny + iyn;
+        bool reflected = false;
+        if (hit ? first_face : corner) {
             // first solid face crossed (trench_charging_2d.py:512-539) in cell units
-            const int y0c = iy0 < 0 ? 0 : iy0;
-            const int diy_e = (iyn) - y0c;   // both rows clipped like the reference
-            if (hit || diy_e != 0) {
-                const float inf = __int_as_float(0x7f800000);
-                const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - ox0) / sx : inf;
-                const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - oy0) / sy : inf;
-                const bool x_first = fx < fy;
-                const int xn = ix;  // already wrapped ix0 + dix
-                const int ax_ = x_first ? xn : ix0, ay_ = x_first ? y0c : y0c + diy_e;
-                const bool use_last = dix != 0 && diy_e != 0 && F.vac(ax_ * ny + ay_);
-                const int cx = use_last ? xn : ax_, cy = use_last ? y0c + diy_e : ay_;
-                const bool face_x = use_last ? !x_first : x_first;
-                const int ccell = cx * ny + cy;
-                hit = !F.vac(ccell);
-                dcell = ccell;
-                if (hit && barrier) {
-                    const float4 b = __ldg(k.barrier + ccell);
-                    // neighbour the particle came from: W/E across an x face, S/N across a y face
-                    const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
-                    const float vn = face_x ? vx : vy;
-                    if (0.5f * vn * vn < qm * dphi) {
-                        if (face_x) vx = -vx; else vy = -vy;
-                        ix = ix0; iy = iy0; ox = ox0; oy = oy0;
-                        hit = false;
-                    }
+            const float inf = __int_as_float(0x7f800000);
+            const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - ox) / sx : inf;
+            const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - oy) / sy : inf;
+            const bool x_first = fx < fy;
+            const int ax_ = x_first ? nix : ix, ay_ = x_first ? y0c : y0c + diy_e;
+            const bool use_last = dix != 0 && diy_e != 0 && F.vac(ax_ * ny + ay_);
+            const int cx = use_last ? nix : ax_, cy = use_last ? y0c + diy_e : ay_;
+            const bool face_x = use_last ? !x_first : x_first;
+            const int ccell = cx * ny + cy;
+            hit = !F.vac(ccell);
+            dcell = ccell;
+            if (hit && barrier) {
+                const float4 b = __ldg(k.barrier + ccell);
+                // neighbour the particle came from: W/E across an x face, S/N across a y face
+                const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
+                const float vn = face_x ? vxn : vyn;
+                if (0.5f * vn * vn < qm * dphi) {
+                    // reflect: normal velocity flips, position returns to the vacuum start point
+                    vx = face_x ? -vxn : vxn;
+                    vy = face_x ? vyn : -vyn;
+                    hit = false;
+                    reflected = true;
                 }
             }
         }
+        if (!reflected) { ix = nix; iy = niy; ox = nox; oy = noy; vx = vxn; vy = vyn; }
 
         int done = 0;
         if (hit) {
@@ -246,7 +258,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
             if (a.d_hit) a.d_hit[pid] = dcell;
             if (spc == 0) ++my_hit_i; else ++my_hit_e;
             done = 1;
-        } else if (escaped) {
+        } else if (escaped && !reflected) {
             if (spc == 0) ++my_esc_i; else ++my_esc_e;
             done = 2;
         } else if (steps >= stop_at) {
@@ -353,6 +365,8 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.dx = ctx->dx;
     k.vscale = ctx->vscale;
     k.inv_v = (float)(1.0 / ctx->vscale);
+    k.inv_dx = 1.0 / ctx->dx;
+    k.inv_v64 = 1.0 / ctx->vscale;
     k.field = ctx->d_field;
     k.barrier = ctx->d_barrier;
     k.queue = ctx->d_queue;
