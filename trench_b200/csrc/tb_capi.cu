@@ -68,7 +68,7 @@ extern "C" int tb_create(tb_ctx **out, int device, int nx, int ny, double dx, co
     const size_t cells = (size_t)nx * ny;
     const size_t padded = (cells + 1) & ~(size_t)1;
     e = cudaMalloc(&c->d_vac, cells);
-    if (e == cudaSuccess) e = cudaMalloc(&c->d_field, padded * sizeof(tb_fcell));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_field, (size_t)tb_halo_count(nx, ny) * sizeof(tb_fcell));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_barrier, padded * sizeof(float4));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_queue, 8 * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));

@@ -19,6 +19,56 @@ struct __align__(8) tb_fcell {
     float ex, ey;
 };
 
+// Packed FP32 field with a one-cell halo: padded cell (i, j), i in [-1, nx],
+// j in [-1, ny], lives at (i + 1) * (ny + 2) + (j + 1).  Column -1 repeats
+// column nx-1 and column nx repeats column 0 (x periodic); row -1 repeats row 0
+// and row ny repeats row ny-1 (the reference clips y indices,
+// trench_charging_2d.py:502-505).  Bilinear corners then need no wrap or clip.
+__host__ __device__ __forceinline__ int tb_halo_count(int nx, int ny) {
+    const int n = (nx + 2) * (ny + 2);
+    return (n + 1) & ~1;  // even count: whole 16-byte units for the bulk copy
+}
+
+// True if cell (ix, iy) and its 8 neighbours (x periodic, rows clipped to the grid
+// like the reference's cell lookups) are all vacuum: a move of less than one cell
+// from such a cell cannot reach a solid cell.
+__device__ __forceinline__ bool tb_interior(const uint8_t *vac, int nx, int ny, int ix, int iy) {
+    for (int a = -1; a <= 1; ++a) {
+        const int i = ix + a < 0 ? nx - 1 : (ix + a >= nx ? 0 : ix + a);
+        for (int b = -1; b <= 1; ++b) {
+            const int j = iy + b < 0 ? 0 : (iy + b > ny - 1 ? ny - 1 : iy + b);
+            if (!vac[i * ny + j]) return false;
+        }
+    }
+    return true;
+}
+
+// Packed tracer cell: E*vac scaled to cell units, bit 0 of ex = vacuum, bit 0 of
+// ey = interior (one-ulp perturbations of FP32 values; a flagged zero becomes the
+// smallest denormal, which flushes to zero in the tracer's arithmetic).
+__device__ __forceinline__ tb_fcell tb_pack_cell(double ex, double ey, bool vacuum, bool interior, double scale) {
+    const double v = vacuum ? 1.0 : 0.0;
+    uint32_t bx = __float_as_uint((float)(ex * v * scale));
+    uint32_t by = __float_as_uint((float)(ey * v * scale));
+    bx = vacuum ? (bx | 1u) : (bx & ~1u);
+    by = interior ? (by | 1u) : (by & ~1u);
+    return tb_fcell{__uint_as_float(bx), __uint_as_float(by)};
+}
+
+// Writes the packed value of cell (ix, iy) and its halo copies.
+__device__ __forceinline__ void tb_store_halo(tb_fcell *out, int nx, int ny, int ix, int iy, tb_fcell v) {
+    const int P = ny + 2;
+    int cs[3], rs[3], nc = 0, nr = 0;
+    cs[nc++] = ix + 1;
+    if (ix == nx - 1) cs[nc++] = 0;
+    if (ix == 0) cs[nc++] = nx + 1;
+    rs[nr++] = iy + 1;
+    if (iy == 0) rs[nr++] = 0;
+    if (iy == ny - 1) rs[nr++] = ny + 1;
+    for (int a = 0; a < nc; ++a)
+        for (int b = 0; b < nr; ++b) out[cs[a] * P + rs[b]] = v;
+}
+
 struct tb_poisson;
 void tb_poisson_free(tb_poisson *ps);
 

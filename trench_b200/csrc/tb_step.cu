@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(ONE_BLOCK) k_finish(const tb_step_desc d, cons
 // K5: E = -grad phi over vacuum neighbours (trench_charging_2d.py:429-454), the
 // packed FP32 tracer field, the per-face wall barrier and the probe history.
 __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac, double scale_e, double scale_phi,
-                        tb_fcell *out, float4 *bar, int padded) {
+                        tb_fcell *out, float4 *bar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = nx * ny;
     if (c == 0) {
@@ -167,8 +167,7 @@ __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac
             for (int k = 0; k < d.n_probes; ++k)
                 d.d_hist[(size_t)row * d.hist_cols + H_PROBE0 + k] = d.d_phi[d.d_probes[k]];
     }
-    if (c >= padded) return;
-    if (c >= n) { out[c] = tb_fcell{0.f, 0.f}; return; }
+    if (c >= n) return;
     const int ix = c / ny, iy = c - ix * ny;
     const int w = (ix == 0 ? nx - 1 : ix - 1) * ny + iy, e = (ix == nx - 1 ? 0 : ix + 1) * ny + iy;
     const double *phi = d.d_phi;
@@ -196,11 +195,7 @@ __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac
     const double ex = -gx, ey = -gy;
     if (d.d_ex) { d.d_ex[c] = ex; d.d_ey[c] = ey; }
     const int v = vac[c] ? 1 : 0;
-    const float fx = (float)(ex * (double)v * scale_e);
-    const float fy = (float)(ey * (double)v * scale_e);
-    uint32_t bx = __float_as_uint(fx);
-    bx = v ? (bx | 1u) : (bx & ~1u);
-    out[c] = tb_fcell{__uint_as_float(bx), fy};
+    tb_store_halo(out, nx, ny, ix, iy, tb_pack_cell(ex, ey, v, v && tb_interior(vac, nx, ny, ix, iy), scale_e));
     float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!v && d.d_wface) {
         const double f = d.d_wface[c];
@@ -253,10 +248,10 @@ extern "C" int tb_step_potential(tb_ctx *ctx, const tb_step_desc *d, void *strea
     else
         k_gemv<double><<<blocks, threads, 0, s>>>(d->n_rows, d->m, d->d_green64, d->d_rho_s, d->d_phi, d->d_ext,
                                                   d->d_rows);
-    const int cells = ctx->nx * ctx->ny, padded = (cells + 1) & ~1;
+    const int cells = ctx->nx * ctx->ny;
     const double scale_e = ctx->dx / (d->vscale * d->vscale), scale_phi = 1.0 / (d->vscale * d->vscale);
-    k_field<<<(padded + 255) / 256, 256, 0, s>>>(*d, ctx->nx, ctx->ny, ctx->d_vac, scale_e, scale_phi, ctx->d_field,
-                                                ctx->d_barrier, padded);
+    k_field<<<(cells + 255) / 256, 256, 0, s>>>(*d, ctx->nx, ctx->ny, ctx->d_vac, scale_e, scale_phi, ctx->d_field,
+                                               ctx->d_barrier);
     TB_CUDA(ctx, cudaGetLastError());
     ctx->vscale = d->vscale;
     ctx->fields_ready = 1;

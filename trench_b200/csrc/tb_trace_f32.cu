@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
     const tb_trace_args &a = k.a;
     const int nx = k.nx, ny = k.ny;
     const int cells = nx * ny;
+    const int P = ny + 2;  // padded column stride
 
     FieldView<SMEM> F;
     if (SMEM) {
@@ -122,12 +123,13 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
     const bool tapered = a.tapered != 0;
     const bool first_face = barrier || tapered;
 
-    long long pid = -1;
+    // Particle state: cell (ix, iy) and FP32 offset (ox, oy) in [0,1) cell units.
+    // ix in [0, nx-1]; iy >= -1 in practice (below the grid only over a vacuum bottom row).
+    int pid = -1;
     int ix = 0, iy = 0, steps = 0, stop_at = 0, spc = 0;
     float ox = 0.f, oy = 0.f, vx = 0.f, vy = 0.f, qm = 0.f;
     bool open = true;
-    unsigned long long my_steps = 0;
-    unsigned my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
+    unsigned my_steps = 0, my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
 
     for (;;) {
         // One ballot per iteration: refill empty lanes from the global queue (one
@@ -146,10 +148,12 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
                 if (pid < 0) {
                     const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
                     if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
-                        pid = (long long)idx;
+                        pid = (int)idx;
+                        // metres -> cells: x lies in cell min(int(x/dx), nx-1) as in the
+                        // reference (trench_charging_2d.py:611)
                         const double xc = a.d_x[pid] * k.inv_dx, yc = a.d_y[pid] * k.inv_dx;
                         ix = min(max((int)xc, 0), nx - 1);
-                        iy = (int)floor(yc);
+                        iy = min((int)floor(yc), ny - 1);  // a start above the grid escapes at once
                         ox = fminf(fmaxf((float)(xc - (double)ix), 0.f), ONE_BELOW);
                         oy = fminf(fmaxf((float)(yc - (double)iy), 0.f), ONE_BELOW);
                         vx = (float)(a.d_vx[pid] * k.inv_v64);
@@ -164,51 +168,53 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         }
         if (pid < 0) continue;
 
-        // ---- field at the current position: vacuum-weighted bilinear (branch-free) ----
-        const bool hx = ox >= 0.5f, hy = oy >= 0.5f;
+        // ---- vacuum-weighted bilinear field (trench_charging_2d.py:492-509) ----
+        // corners (i0, j0) = (ix - 1 + hx, iy - 1 + hy) .. (i0 + 1, j0 + 1); in the halo-padded
+        // field i0 + 1 = ix + hx needs no wrap and the clipped rows need one clamp
+        const int hx = ox >= 0.5f ? 1 : 0, hy = oy >= 0.5f ? 1 : 0;
         const float tx = hx ? ox - 0.5f : ox + 0.5f;
         const float ty = hy ? oy - 0.5f : oy + 0.5f;
-        int i0 = hx ? ix : ix - 1;
-        i0 = i0 < 0 ? nx - 1 : i0;
-        int i1 = hx ? ix + 1 : ix;
-        i1 = i1 >= nx ? 0 : i1;
-        const int j0 = min(max(hy ? iy : iy - 1, 0), ny - 1);
-        const int j1 = min(max(hy ? iy + 1 : iy, 0), ny - 1);
-        const int r0 = i0 * ny, r1 = i1 * ny;
-        const tb_fcell c00 = F.at(r0 + j0), c10 = F.at(r1 + j0);
-        const tb_fcell c01 = F.at(r0 + j1), c11 = F.at(r1 + j1);
+        const int base = (ix + hx) * P + max(iy + hy, 0);
+        const tb_fcell c00 = F.at(base), c01 = F.at(base + 1);
+        const tb_fcell c10 = F.at(base + P), c11 = F.at(base + P + 1);
         const float ux = 1.f - tx, uy = 1.f - ty;
         const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
         const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
         const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
         const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
-        const float qs = qm / fmaxf(sw, 1e-12f);
+        const float qs = __fdividef(qm, fmaxf(sw, 1e-12f));
         const float ax = qs * sex, ay = qs * sey;
+        // the start cell is the corner on the particle's side of each centre line; its
+        // interior flag says every 8-neighbour is vacuum, so a move of < 1 cell cannot
+        // touch a wall and the end-cell and corner checks are skipped
+        const float start_ey = hx ? (hy ? c00.ey : c01.ey) : (hy ? c10.ey : c11.ey);
+        const bool near = !(__float_as_uint(start_ey) & 1u);
 
-        // ---- CFL step and trapezoid update ----
+        // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
         const float speed = sqrtf(vx * vx + vy * vy);
         const float acc = sqrtf(ax * ax + ay * ay);
-        const float dt = cfl / (speed + sqrtf(2.f * acc) + k.inv_v);
+        const float dt = __fdividef(cfl, speed + sqrtf(2.f * acc) + k.inv_v);
         const float vxn = vx + ax * dt, vyn = vy + ay * dt;
         const float sx = 0.5f * (vx + vxn) * dt, sy = 0.5f * (vy + vyn) * dt;
         float nox = ox + sx, noy = oy + sy;
-        const int dix = (nox >= 1.f) ? 1 : ((nox < 0.f) ? -1 : 0);
-        const int diy = (noy >= 1.f) ? 1 : ((noy < 0.f) ? -1 : 0);
-        nox = dix > 0 ? nox - 1.f : (dix < 0 ? nox + 1.f : nox);
-        noy = diy > 0 ? noy - 1.f : (diy < 0 ? noy + 1.f : noy);
-        nox = fminf(nox, ONE_BELOW);
-        noy = fminf(noy, ONE_BELOW);
+        const bool gx = nox >= 1.f, lx = nox < 0.f, gy = noy >= 1.f, ly = noy < 0.f;
+        const int dix = gx ? 1 : (lx ? -1 : 0);
+        const int diy = gy ? 1 : (ly ? -1 : 0);
+        nox = fminf(gx ? nox - 1.f : (lx ? nox + 1.f : nox), ONE_BELOW);
+        noy = fminf(gy ? noy - 1.f : (ly ? noy + 1.f : noy), ONE_BELOW);
         int nix = ix + dix;
         nix = nix < 0 ? nx - 1 : (nix >= nx ? 0 : nix);
         const int niy = iy + diy;
         ++steps;
         ++my_steps;
         const bool escaped = niy >= ny;
-        const int iyn = min(max(niy, 0), ny - 1);
-        const int y0c = min(max(iy, 0), ny - 1);
-        const int diy_e = iyn - y0c;   // row change with both rows clipped like the reference
-        const bool hit_end = !escaped && !F.vac(nix * ny + iyn);
-        const bool corner = tapered && !escaped && !hit_end && dix != 0 && diy_e != 0;
+        bool hit_end = false, corner = false;
+        if (near && !escaped) {
+            hit_end = !F.vac((nix + 1) * P + max(niy, -1) + 1);
+            // both the column and the (clipped) row changed: a staircase corner may lie on
+            // the path between two vacuum cells (trench_charging_2d.py:614-621)
+            corner = tapered && !hit_end && dix != 0 && max(niy, 0) != max(iy, 0);
+        }
 
         if (!(hit_end || corner || escaped || steps >= stop_at)) {
             ix = nix; iy = niy; ox = nox; oy = noy; vx = vxn; vy = vyn;
@@ -216,6 +222,9 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         }
 
         // ---- rare path: wall contact, escape, or step cap ----
+        const int y0c = min(max(iy, 0), ny - 1);
+        const int iyn = min(max(niy, 0), ny - 1);
+        const int diy_e = iyn - y0c;     // rows clipped like the reference
         bool hit = hit_end;
         int dcell = nix * ny + iyn;
         bool reflected = false;
@@ -226,11 +235,11 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
             const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - oy) / sy : inf;
             const bool x_first = fx < fy;
             const int ax_ = x_first ? nix : ix, ay_ = x_first ? y0c : y0c + diy_e;
-            const bool use_last = dix != 0 && diy_e != 0 && F.vac(ax_ * ny + ay_);
+            const bool use_last = dix != 0 && diy_e != 0 && F.vac((ax_ + 1) * P + ay_ + 1);
             const int cx = use_last ? nix : ax_, cy = use_last ? y0c + diy_e : ay_;
             const bool face_x = use_last ? !x_first : x_first;
             const int ccell = cx * ny + cy;
-            hit = !F.vac(ccell);
+            hit = !F.vac((cx + 1) * P + cy + 1);
             dcell = ccell;
             if (hit && barrier) {
                 const float4 b = __ldg(k.barrier + ccell);
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
                 const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
                 const float vn = face_x ? vxn : vyn;
                 if (0.5f * vn * vn < qm * dphi) {
-                    // reflect: normal velocity flips, position returns to the vacuum start point
+                    // reflect: the normal velocity flips, the position stays at the start point
                     vx = face_x ? -vxn : vxn;
                     vy = face_x ? vyn : -vyn;
                     hit = false;
@@ -292,32 +301,24 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         if (my_esc_i) atomicAdd(t + 0, (unsigned long long)my_esc_i);
         if (my_esc_e) atomicAdd(t + 1, (unsigned long long)my_esc_e);
         if (my_lost) atomicAdd(t + 2, (unsigned long long)my_lost);
-        if (my_steps) atomicAdd(t + 3, my_steps);
+        if (my_steps) atomicAdd(t + 3, (unsigned long long)my_steps);
         if (my_hit_i) atomicAdd(t + 4, (unsigned long long)my_hit_i);
         if (my_hit_e) atomicAdd(t + 5, (unsigned long long)my_hit_e);
     }
 }
 
-// Packs FP64 fields into the FP32 tracer layout; one thread per cell.
+// Packs FP64 fields into the halo-padded FP32 tracer layout; one thread per cell.
 __global__ void pack_fields_kernel(int nx, int ny, double scale_e, double scale_phi, const uint8_t *vac,
                                    const double *ex, const double *ey, const double *phi,
-                                   const double *wface, tb_fcell *out, float4 *bar, int padded) {
+                                   const double *wface, tb_fcell *out, float4 *bar) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int cells = nx * ny;
-    if (c >= padded) return;
-    if (c >= cells) {
-        out[c] = tb_fcell{0.f, 0.f};
-        return;
-    }
+    if (c >= cells) return;
+    const int ix = c / ny, iy = c - ix * ny;
     const int v = vac[c] ? 1 : 0;
-    const float fx = (float)(ex[c] * (double)v * scale_e);
-    const float fy = (float)(ey[c] * (double)v * scale_e);
-    uint32_t bx = __float_as_uint(fx);
-    bx = v ? (bx | 1u) : (bx & ~1u);
-    out[c] = tb_fcell{__uint_as_float(bx), fy};
+    tb_store_halo(out, nx, ny, ix, iy, tb_pack_cell(ex[c], ey[c], v, v && tb_interior(vac, nx, ny, ix, iy), scale_e));
     float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!v && phi != nullptr) {
-        const int ix = c / ny, iy = c - ix * ny;
         const int w = (ix == 0 ? nx - 1 : ix - 1) * ny + iy;
         const int e = (ix == nx - 1 ? 0 : ix + 1) * ny + iy;
         const double f = wface[c], pc = phi[c];
@@ -334,13 +335,11 @@ __global__ void pack_fields_kernel(int nx, int ny, double scale_e, double scale_
 int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
                           const double *wface, double vscale, cudaStream_t s) {
     const int cells = ctx->nx * ctx->ny;
-    const int padded = (cells + 1) & ~1;
     const double scale_e = ctx->dx / (vscale * vscale);
     const double scale_phi = 1.0 / (vscale * vscale);
     const int threads = 256;
-    pack_fields_kernel<<<(padded + threads - 1) / threads, threads, 0, s>>>(
-        ctx->nx, ctx->ny, scale_e, scale_phi, ctx->d_vac, ex, ey, phi, wface, ctx->d_field, ctx->d_barrier,
-        padded);
+    pack_fields_kernel<<<(cells + threads - 1) / threads, threads, 0, s>>>(
+        ctx->nx, ctx->ny, scale_e, scale_phi, ctx->d_vac, ex, ey, phi, wface, ctx->d_field, ctx->d_barrier);
     TB_CUDA(ctx, cudaGetLastError());
     ctx->vscale = vscale;
     ctx->fields_ready = 1;
@@ -371,8 +370,7 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.barrier = ctx->d_barrier;
     k.queue = ctx->d_queue;
     k.err = ctx->d_err;
-    const int cells = ctx->nx * ctx->ny;
-    k.bytes = ((cells + 1) & ~1) * (int)sizeof(tb_fcell);
+    k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     long long want = (a->n + F32_THREADS - 1) / F32_THREADS;
@@ -400,7 +398,8 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
 
 namespace {
 
-constexpr size_t NOALLOC_FIELD_BYTES = (size_t)TB_NOALLOC_MAX_CELLS * sizeof(tb_fcell);
+// a grid of at most MAX cells has a halo-padded field of at most 3*MAX + 6 cells
+constexpr size_t NOALLOC_FIELD_BYTES = ((size_t)3 * TB_NOALLOC_MAX_CELLS + 8) * sizeof(tb_fcell);
 constexpr size_t NOALLOC_BARRIER_BYTES = (size_t)TB_NOALLOC_MAX_CELLS * sizeof(float4);
 constexpr size_t NOALLOC_COUNTER_BYTES = 256;
 constexpr size_t NOALLOC_BYTES = NOALLOC_FIELD_BYTES + NOALLOC_BARRIER_BYTES + NOALLOC_COUNTER_BYTES;
