@@ -1,13 +1,15 @@
 """ctypes binding of libtrench_b200.so (the C ABI in include/trench_b200.h).
 
-The library is built in-tree by ``trench_b200.build``.  Loading fails loudly: there
-is no CPU fallback anywhere in this package.
+The library is built in-tree by ``trench_b200.build``; TRENCH_B200_LIB may name
+another build of the same ABI (for comparing kernel variants).  Loading fails
+loudly: there is no CPU fallback anywhere in this package.
 """
 import ctypes
+import os
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-LIB_PATH = HERE / "libtrench_b200.so"
+LIB_PATH = Path(os.environ.get("TRENCH_B200_LIB", HERE / "libtrench_b200.so"))
 
 TB_OK = 0
 TB_ERR_ARG = 1
