@@ -176,7 +176,7 @@ int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
  * not let cudaMalloc/cudaFree synchronise the device -- this entry point allocates
  * nothing and needs no context: the tracer's scratch (packed FP32 field, wall
  * barrier, work-queue counter, check flag) lives in a static device array of about
- * 1.5 MiB that every GPU loading the library holds until the process exits.  It
+ * 2.5 MiB that every GPU loading the library holds until the process exits.  It
  * traces like tb_trace with TB_PRECISION_F32 on the current device; the caller
  * passes the device vacuum mask d_vac (nx*ny bytes, 1 = vacuum), the FP64 fields
  * in args->d_ex/d_ey (and d_phi/d_wface for the barrier model) and every input and

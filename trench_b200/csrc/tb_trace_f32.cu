@@ -394,7 +394,7 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
 // tb_trace_f32_noalloc keeps the tracer's scratch -- the packed FP32 field, the
 // per-face wall barrier, the work-queue counter and the check flag -- in the
 // file-scope array below instead of a context.  Every GPU that loads this
-// library holds the array (about 1.5 MiB) until the process exits.
+// library holds the array (about 2.5 MiB) until the process exits.
 
 namespace {
 
