@@ -344,6 +344,56 @@ def run_b200(args, p):
     return 0
 
 
+def run_sweep(args):
+    """Batched sweep: 64 uneven cases advanced together, one persistent tracer launch per
+    batch (configuration 3); reported as particles/s over all cases."""
+    import torch
+    from trench_b200 import inject
+    from trench_b200.batch import ChargingBatch, sweep_params
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    ps, seps = sweep_params(args.cases, seed=0)
+    t0 = time.perf_counter()
+    batch = ChargingBatch(ps, device=0, max_batches=args.warmup + args.steps + 4)
+    setup_s = time.perf_counter() - t0
+    rng = np.random.default_rng(11)
+    total = 0
+    for i, (p, sep) in enumerate(zip(ps, seps)):
+        energy = inject.mixture_energy([(0.5, "normal", 40.0, 6.0), (0.5, "normal", 40.0 + sep, 6.0)])
+        sampler = inject.energy_angle_sampler(p, energy, inject.half_gaussian_angle(3.0))
+        batch.load(i, *inject.inject(p, p.n_per_batch, batch.cases[i].ny, rng, ion_velocity=sampler))
+        total += 2 * p.n_per_batch
+    batch.step()
+    torch.cuda.synchronize()
+    batch.capture()
+    for _ in range(args.warmup - 1):
+        batch.replay()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.replay()
+        e1.record()
+        flush.zero_()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    batch.check()
+    steps_per_batch = sum(c.history()["particle_steps"][-1] for c in batch.cases)
+    line = {"metric": METRIC, "value": total / (np.mean(ms) / 1000.0), "unit": "particles/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(ms)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"batched sweep: {len(ps)} cases, widths 12-40, depths 40-200, tapers -3..5 deg, "
+                                   "mask conductive/dielectric, particles/species log-uniform 2^15-2^17, "
+                                   "bimodal IED separation 30-150 eV", "cases": len(ps),
+                       "particles_per_batch": total, "setup_s": setup_s},
+            "batches_per_s": 1000.0 / float(np.mean(ms)), "particle_steps_per_batch": float(steps_per_batch)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def case_smem_peak(case):
     """Shared-memory load bandwidth measured on this GPU (GB/s)."""
     import ctypes
@@ -361,9 +411,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--particles", type=int, default=1 << 19, help="particles per species per batch")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample duration")
+    ap.add_argument("--workload", default="ar8", choices=["ar8", "sweep"],
+                    help="ar8: the AR-8 RF-charging case (default); sweep: many uneven cases per launch")
+    ap.add_argument("--cases", type=int, default=64, help="cases of the sweep workload")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.workload == "sweep":
+        return run_sweep(args)
     p = workload(args.particles)
     if args.impl == "reference":
         return run_reference(args, p)

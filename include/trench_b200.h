@@ -170,6 +170,23 @@ int tb_step_charge(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
  * tb_set_fields) and probe history. */
 int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
 
+/* ---- Case packs: many trench cases in one persistent FP32 launch -----------------
+ * A pack groups contexts of one device (different grids allowed).  tb_pack_set_args
+ * takes one tb_trace_args per case (FP32 rules of tb_trace; the cases' fields must
+ * have been packed) and is synchronous; tb_pack_trace launches one persistent kernel
+ * whose CTAs pick the case with the most unclaimed particles, stage its field in
+ * shared memory and trace from its queue, so cases of uneven size share all SMs.
+ * reset != 0 first sets status = live, steps = 0 and zeroes counts and totals of every
+ * case.  No counterpart in the reference, which runs cases one after another. */
+typedef struct tb_pack tb_pack;
+int tb_pack_create(tb_pack **out, int n_cases, tb_ctx *const *ctxs);
+int tb_pack_destroy(tb_pack *pack);
+const char *tb_pack_last_error(const tb_pack *pack);
+int tb_pack_set_args(tb_pack *pack, const tb_trace_args *args);
+int tb_pack_trace(tb_pack *pack, int reset, void *stream);
+/* Synchronise `stream`, then read and clear the pack's device check flag. */
+int tb_pack_check(tb_pack *pack, void *stream);
+
 /* ---- No-allocation FP32 tracer ---------------------------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc -- a
  * host application whose memory pool owns all device memory, or a caller that must

@@ -173,6 +173,28 @@ def main(ref):
              solid=res["solid"], mask=res["mask"],
              **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
 
+    # circuit_rf batch loop with the reference's test waveform (tests/test_taper.py:273-283)
+    rfrun = replace(taper, bias="rf", field_mode="circuit_rf", side_bc="pillar", rf_freq=5e8, sigma_s=1e-14,
+                    n_batches=3, wall_model="barrier")
+    tt = np.arange(256) / 256 / rfrun.rf_freq
+    circ = dict(t=tt, uw=-60 - 20 * np.sin(2 * np.pi * tt * rfrun.rf_freq),
+                um=-30 - 10 * np.sin(2 * np.pi * tt * rfrun.rf_freq), up=tt * 0,
+                V1=30 + 10 * np.sin(2 * np.pi * tt * rfrun.rf_freq), E=np.array([]),
+                us=-60 - 20 * np.sin(2 * np.pi * tt * rfrun.rf_freq), i=tt * 0, cached=False, ied_model="instant",
+                sheath=None, n_periods=1, elements={}, ied_computed=False, s=1e-5, tau_i=1e-9)
+    import copy
+    orig_solve, orig_summary = T.PC.solve_circuit_cached, T.PC.summary
+    T.PC.solve_circuit_cached = lambda *a, **k: copy.deepcopy(circ)
+    T.PC.summary = lambda c: "test circuit"
+    try:
+        res = T.run(rfrun, log=lambda s: None)
+    finally:
+        T.PC.solve_circuit_cached, T.PC.summary = orig_solve, orig_summary
+    save("run_rf_taper.npz", params=params_json(rfrun), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
+         solid=res["solid"], mask=res["mask"], circuit_t=circ["t"], circuit_uw=circ["uw"], circuit_um=circ["um"],
+         circuit_up=circ["up"], circuit_V1=circ["V1"],
+         **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
+
     # --- field-side cases -----------------------------------------------------
     for name, p in {"floating": runs["floating_leak"], "fixed": runs["fixed_leak"],
                     "dielectric": runs["dielectric_leak"],

@@ -75,3 +75,16 @@ def test_samplers_shapes_and_ranges():
     assert (vy < 0).all()
     ang = np.degrees(np.arctan2(vx, -vy))
     assert 2.0 < np.std(ang) < 4.0 and abs(np.mean(ang)) < 0.2
+
+
+def test_sweep_cases_are_valid_and_spread():
+    from trench_b200.batch import sweep_params
+    ps, seps = sweep_params(64, seed=0)
+    assert len(ps) == 64
+    for p in ps:
+        geometry.build_geometry(p)       # every drawn geometry is valid
+        assert 12 <= p.trench_w <= 40 and 40 <= p.trench_d <= 200 and -3 <= p.trench_taper_deg <= 5
+        assert 2 ** 15 - 1 <= p.n_per_batch <= 2 ** 17 + 1
+    kinds = {p.mask_type for p in ps}
+    assert kinds == {"conductor", "dielectric"}
+    assert 30 <= min(seps) and max(seps) <= 150

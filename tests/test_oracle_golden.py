@@ -120,3 +120,28 @@ def test_oracle_conductor_step_matches_reference():
     g = load_golden("conductor_step.npz")
     got = [OF.conductor_step(*a) for a in g["args"]]
     np.testing.assert_allclose(got, g["values"], rtol=1e-14, atol=0)
+
+
+def circuit_of(g):
+    return dict(t=g["circuit_t"], uw=g["circuit_uw"], um=g["circuit_um"], up=g["circuit_up"], V1=g["circuit_V1"])
+
+
+def test_oracle_rf_batch_loop_matches_reference_run():
+    """circuit_rf: RF basis, stratified launch phases and in-flight clock
+    (trench_charging_2d.py:1079, 1231-1234) reproduce the reference run()."""
+    g = load_golden("run_rf_taper.npz")
+    p = g["p"]
+    solid, mask, _, _ = geometry.build_geometry(p)
+    st = OF.BatchState(p, solid, mask, circuit_of(g))
+    rng = np.random.default_rng(p.seed)
+    phase = np.random.default_rng(np.random.SeedSequence([p.seed, 0x5246]))
+    period = st.fields["rf"]["period"]
+    for _ in range(p.n_batches):
+        parts = inject.inject(p, p.n_per_batch, solid.shape[1], rng, lambda r, k: np.full(k, p.electron_temp_eV / 2))
+        rf = {**st.fields["rf"], "initial_time": np.concatenate(
+            [inject.launch_times(phase, p.n_per_batch, period) for _ in range(2)])}
+        st.step(*OT.trace(*parts, st.Ex, st.Ey, ~solid, p, st.barrier(), rf=rf))
+    np.testing.assert_allclose(st.rho, g["rho_raw"], rtol=1e-12, atol=1e-6)
+    np.testing.assert_allclose(st.phi, g["mean_phi"], rtol=0, atol=1e-9)
+    for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
+        np.testing.assert_array_equal(np.array(st.hist[k]), g[f"hist_{k}"])

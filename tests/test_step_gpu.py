@@ -150,3 +150,17 @@ def test_graph_replay_equals_eager(case_cls):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(a.rho(), b.rho())
     np.testing.assert_array_equal(a.history()["ratio_i_bottom"], b.history()["ratio_i_bottom"])
+
+
+def test_rf_batch_loop_matches_reference_run(case_cls):
+    """circuit_rf on the device: basis fields, launch phases and the in-flight clock
+    (FP64 kernel) reproduce the reference run() (tests/test_taper.py:273-294)."""
+    g = load_golden("run_rf_taper.npz")
+    p = g["p"]
+    circuit = dict(t=g["circuit_t"], uw=g["circuit_uw"], um=g["circuit_um"], up=g["circuit_up"], V1=g["circuit_V1"])
+    case = case_cls(p, precision="f32", green="f64", circuit=circuit)
+    res = case.run()
+    np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-6)
+    np.testing.assert_allclose(res["mean_phi"], g["mean_phi"], rtol=1e-10, atol=1e-8)
+    for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
+        np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])

@@ -93,6 +93,12 @@ SIGNATURES = {
     "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
+    "tb_pack_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
+    "tb_pack_destroy": (ctypes.c_int, [_vp]),
+    "tb_pack_last_error": (ctypes.c_char_p, [_vp]),
+    "tb_pack_set_args": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs)]),
+    "tb_pack_trace": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
+    "tb_pack_check": (ctypes.c_int, [_vp, _vp]),
     "tb_trace_f32_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dbl, _vp, ctypes.POINTER(TraceArgs),
                                             _dbl, _vp]),
 }

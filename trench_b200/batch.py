@@ -1,0 +1,142 @@
+"""ChargingBatch: many independent trench cases advanced together.
+
+All cases' particles are traced by one persistent launch (``tb_pack_trace``: CTAs
+move between cases by remaining work, so uneven cases share every SM); the
+per-case charge, leakage, conductor, potential and field updates follow, and a
+whole batch of all cases can be captured as one CUDA graph.  The reference runs
+such a sweep as one ``run()`` per case (trench_charging_2d.py:1045).
+
+``sweep_params`` draws the sweep workload of uneven cases (widths, depths,
+tapers, mask types and particle counts).
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _capi, geometry
+from .params import Params
+from .step import ChargingCase
+from .tracer import _ptr
+
+
+def sweep_params(n_cases, seed=0, base=None):
+    """Cases with trench width U[12,40] cells, depth U[40,200], sidewall taper
+    U[-3,5] deg, conductive or dielectric mask (equal odds), nx = width + 40,
+    particles per species log-uniform in [2^15, 2^17].  Draws that close the
+    opening are redrawn.  Returns (params list, per-case ion peak separations in eV)."""
+    from dataclasses import replace
+    rng = np.random.default_rng(seed)
+    base = base or Params()
+    out, seps = [], []
+    while len(out) < n_cases:
+        w = int(rng.integers(12, 41))
+        d = int(rng.integers(40, 201))
+        taper = float(rng.uniform(-3.0, 5.0))
+        mask = "conductor" if rng.random() < 0.5 else "dielectric"
+        n = int(round(2 ** rng.uniform(15, 17)))
+        sep = float(rng.uniform(30.0, 150.0))
+        p = replace(base, nx=w + 40, trench_w=w, trench_d=d, trench_taper_deg=taper, floor_t=10, mask_t=20,
+                    n_vac=50, mask_type=mask, mask_eps_r=3.0, field_mode="floating", bias="rf",
+                    electron_temp_eV=3.0, sigma_s=1e-15, n_per_batch=n, seed=int(rng.integers(1 << 30)))
+        try:
+            geometry.build_geometry(p)
+        except ValueError:
+            continue
+        out.append(p)
+        seps.append(sep)
+    return out, seps
+
+
+class ChargingBatch:
+    def __init__(self, params, device=0, green="f64", max_batches=None):
+        if not params:
+            raise ValueError("a batch needs at least one case")
+        self.dev = torch.device("cuda", int(device))
+        self.cases = [ChargingCase(p, device=device, precision="f32", green=green, max_batches=max_batches)
+                      for p in params]
+        L = _capi.lib()
+        handles = (ctypes.c_void_p * len(self.cases))(*[c.ctx.handle.value for c in self.cases])
+        h = ctypes.c_void_p()
+        code = L.tb_pack_create(ctypes.byref(h), len(self.cases), handles)
+        if code != _capi.TB_OK:
+            _capi.raise_for(code, None)
+        self.pack = h
+        self.n_loaded = [0] * len(self.cases)
+        self._graph = None
+        self._args_for = None
+
+    def _check(self, code):
+        if code != _capi.TB_OK:
+            msg = _capi.lib().tb_pack_last_error(self.pack).decode(errors="replace")
+            if code == _capi.TB_ERR_ARG:
+                raise ValueError(msg)
+            raise _capi.TBError(code, msg)
+
+    def close(self):
+        if getattr(self, "pack", None):
+            _capi.lib().tb_pack_destroy(self.pack)
+            self.pack = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, i, x, y, vx, vy, qm, spc, non_blocking=False):
+        self.cases[i].load(x, y, vx, vy, qm, spc, non_blocking=non_blocking)
+        self.n_loaded[i] = len(x)
+
+    def _set_args(self):
+        key = tuple(self.n_loaded)
+        if self._args_for == key:
+            return
+        arr = (_capi.TraceArgs * len(self.cases))()
+        for a, c, n in zip(arr, self.cases, self.n_loaded):
+            p = c.p
+            a.n = n
+            a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in c.X)
+            a.d_spc = _ptr(c.SPC)
+            bar = p.wall_model == "barrier"
+            a.d_phi, a.d_wface = (_ptr(c.phi), _ptr(c.t_wface)) if bar else (None, None)
+            a.max_steps = a.step_budget = int(p.max_steps)
+            a.cfl = float(p.cfl)
+            a.tapered = int(bool(p.trench_taper_deg or (p.mask_t > 0 and p.mask_taper_deg)))
+            a.d_counts, a.d_totals = _ptr(c.counts), _ptr(c.totals)
+            a.d_status, a.d_steps = _ptr(c.status), _ptr(c.steps)
+            a.d_hit = None
+            a.write_state = 0
+        self._check(_capi.lib().tb_pack_set_args(self.pack, arr))
+        self._args_for = key
+
+    def step(self):
+        """One batch of every case on the current stream."""
+        L = _capi.lib()
+        self._set_args()
+        s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        self._check(L.tb_pack_trace(self.pack, 1, s))
+        for c in self.cases:
+            c.ctx.check(L.tb_step_charge(c.ctx.handle, ctypes.byref(c._desc), s))
+            c.ctx.check(L.tb_step_potential(c.ctx.handle, ctypes.byref(c._desc), s))
+
+    def capture(self):
+        self._set_args()
+        side = torch.cuda.Stream(self.dev)
+        side.wait_stream(torch.cuda.current_stream(self.dev))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(g, stream=side):
+                self.step()
+        torch.cuda.current_stream(self.dev).wait_stream(side)
+        self._graph = g
+        return g
+
+    def replay(self):
+        self._graph.replay()
+
+    def check(self):
+        s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        self._check(_capi.lib().tb_pack_check(self.pack, s))
+        for c in self.cases:
+            c.check()

@@ -14,11 +14,12 @@
 // Hierarchy: cell-centred 2x2 aggregation; the coarse operator is one half of
 // the Galerkin product P^T L P for piecewise-constant P restricted to free
 // cells (the scaling that makes aggregation consistent with rediscretisation).
-// Smoother: red-black Gauss-Seidel, forward before and reversed after the
-// coarse correction, so the V-cycle is a symmetric preconditioner.
+// Smoother: multicolour (red-black) Gauss-Seidel, forward before and reversed
+// after the coarse correction, so the V-cycle is a symmetric preconditioner.
 //
 // Many right-hand sides are solved together: vectors are (nrhs, cells) and
-// every kernel covers all of them in one launch (blockIdx.y = rhs).
+// every kernel covers all of them in one launch (blockIdx.y = rhs).  Dot products
+// are per-block partial sums added in block order, so a solve is deterministic.
 #include <math.h>
 
 #include <vector>
@@ -46,6 +47,8 @@ struct tb_poisson {
     double *r64 = nullptr;                     // (max_rhs, n)
     float *e = nullptr, *pr = nullptr, *pz = nullptr, *pp = nullptr, *pq = nullptr;  // PCG vectors
     double *scal = nullptr;                    // (max_rhs, 8) per-rhs scalars
+    double *part = nullptr;                    // (max_rhs, blocks, 2) per-block partial sums
+    int part_blocks = 0;
     int pre = 1, post = 1, coarse_sweeps = 16;
 };
 
@@ -80,9 +83,9 @@ __device__ __forceinline__ double block_sum(double v) {
     return v;
 }
 
-// r64 = b - L x (FP64); scal[S_RR] += |r|^2, scal[S_BB] += |b|^2
+// r64 = b - L x (FP64); per-block partial sums of |r|^2 and |b|^2 into part
 __global__ void k_resid64(int nx, int ny, const double *d, const double *ke, const double *kn, const double *x,
-                          const double *b, double *r, double *scal) {
+                          const double *b, double *r, double *part) {
     const int n = nx * ny, rhs = blockIdx.y;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const double *xr = x + (size_t)rhs * n;
@@ -97,9 +100,20 @@ __global__ void k_resid64(int nx, int ny, const double *d, const double *ke, con
     rr = block_sum(rr);
     bb = block_sum(bb);
     if (threadIdx.x == 0) {
-        atomicAdd(scal + rhs * 8 + S_RR, rr);
-        atomicAdd(scal + rhs * 8 + S_BB, bb);
+        double *pp = part + ((size_t)rhs * gridDim.x + blockIdx.x) * 2;
+        pp[0] = rr;
+        pp[1] = bb;
     }
+}
+
+// scal[rhs][slot0 + j] = sum over blocks of part[rhs][block][j], in block order (deterministic)
+__global__ void k_sum_partials(int nrhs, int nblk, int nslot, const double *part, double *scal, int slot0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrhs * nslot) return;
+    const int rhs = i / nslot, j = i - rhs * nslot;
+    double t = 0;
+    for (int b = 0; b < nblk; ++b) t += part[((size_t)rhs * nblk + b) * 2 + j];
+    scal[rhs * 8 + slot0 + j] = t;
 }
 
 // r32 = r64 / |r64| ; e = 0
@@ -120,14 +134,18 @@ __global__ void k_correct(int n, const float *e, double *x, const double *scal) 
     x[(size_t)rhs * n + c] += nr * (double)e[(size_t)rhs * n + c];
 }
 
-// Red-black Gauss-Seidel half sweep on one colour (x updated in place).
+// Gauss-Seidel sweep over one colour (x updated in place).  Colours 0/1 are the
+// red-black checkerboard; with odd nx the periodic wrap would put columns nx-1 and
+// 0 side by side in one colour, so column nx-1 gets colours 2/3 (by row parity) and
+// no two neighbours ever share a colour.
 __global__ void k_smooth(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
                          float *x, const float *b, int color) {
     const int n = nx * ny, rhs = blockIdx.y;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n) return;
     const int ix = c / ny, iy = c - ix * ny;
-    if (((ix + iy) & 1) != color || fixed[c]) return;
+    const int col = ((nx & 1) && ix == nx - 1) ? 2 + (iy & 1) : ((ix + iy) & 1);
+    if (col != color || fixed[c]) return;
     float *xr = x + (size_t)rhs * n;
     const int w = wrapx(ix - 1, nx) * ny + iy, e = wrapx(ix + 1, nx) * ny + iy;
     float s = b[(size_t)rhs * n + c] + ke[c] * xr[e] + ke[w] * xr[w];
@@ -178,9 +196,9 @@ __global__ void k_prolong(int fnx, int fny, const uint8_t *ffixed, float *x, int
     x[(size_t)rhs * fn + f] += xc[(size_t)rhs * cn + (i >> 1) * cny + (j >> 1)];
 }
 
-// q = L p (FP32, fine level), scal[S_PQ] += p.q
+// q = L p (FP32, fine level); per-block partial sums of p.q into part
 __global__ void k_matvec_dot(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
-                             const float *p, float *q, double *scal) {
+                             const float *p, float *q, double *part) {
     const int n = nx * ny, rhs = blockIdx.y;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     double acc = 0;
@@ -191,7 +209,7 @@ __global__ void k_matvec_dot(int nx, int ny, const float *d, const float *ke, co
         acc = (double)v * (double)p[o + c];
     }
     acc = block_sum(acc);
-    if (threadIdx.x == 0) atomicAdd(scal + rhs * 8 + S_PQ, acc);
+    if (threadIdx.x == 0) part[((size_t)rhs * gridDim.x + blockIdx.x) * 2] = acc;
 }
 
 // x += a p ; r -= a q with a = rz / pq
@@ -205,8 +223,8 @@ __global__ void k_axpy(int n, const float *p, const float *q, float *x, float *r
     r[o] -= a * q[o];
 }
 
-// scal[slot] += r.z
-__global__ void k_dot(int n, const float *r, const float *z, double *scal, int slot) {
+// per-block partial sums of r.z into part
+__global__ void k_dot(int n, const float *r, const float *z, double *part) {
     const int rhs = blockIdx.y, c = blockIdx.x * blockDim.x + threadIdx.x;
     double acc = 0;
     if (c < n) {
@@ -214,7 +232,7 @@ __global__ void k_dot(int n, const float *r, const float *z, double *scal, int s
         acc = (double)r[o] * (double)z[o];
     }
     acc = block_sum(acc);
-    if (threadIdx.x == 0) atomicAdd(scal + rhs * 8 + slot, acc);
+    if (threadIdx.x == 0) part[((size_t)rhs * gridDim.x + blockIdx.x) * 2] = acc;
 }
 
 // p = z + b p with b = rz_new / rz (p = z when first)
@@ -245,6 +263,16 @@ __global__ void k_clear_slots(int nrhs, double *scal, int first, int count) {
 
 dim3 grid_for(int n, int nrhs) { return dim3((n + PT - 1) / PT, nrhs); }
 
+// One colour-ordered Gauss-Seidel sweep, forward (0, 1, 2, 3) or backward.
+void sweep(const Level &L, int nrhs, bool forward, cudaStream_t s) {
+    const dim3 g = grid_for(L.n, nrhs);
+    const int ncol = (L.nx & 1) ? 4 : 2;
+    for (int k = 0; k < ncol; ++k) {
+        const int color = forward ? k : ncol - 1 - k;
+        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, color);
+    }
+}
+
 // z = M r on the fine level (one symmetric V-cycle); r lives in lev[0].b.
 void vcycle(tb_poisson *ps, int l, int nrhs, cudaStream_t s) {
     Level &L = ps->lev[l];
@@ -252,29 +280,17 @@ void vcycle(tb_poisson *ps, int l, int nrhs, cudaStream_t s) {
     k_zero<<<(unsigned)((tot + PT - 1) / PT), PT, 0, s>>>(tot, L.x);
     const dim3 g = grid_for(L.n, nrhs);
     if (l + 1 == (int)ps->lev.size()) {
-        for (int k = 0; k < ps->coarse_sweeps; ++k) {
-            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
-            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
-        }
-        for (int k = 0; k < ps->coarse_sweeps; ++k) {
-            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
-            k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
-        }
+        for (int k = 0; k < ps->coarse_sweeps; ++k) sweep(L, nrhs, true, s);
+        for (int k = 0; k < ps->coarse_sweeps; ++k) sweep(L, nrhs, false, s);
         return;
     }
-    for (int k = 0; k < ps->pre; ++k) {
-        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
-        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
-    }
+    for (int k = 0; k < ps->pre; ++k) sweep(L, nrhs, true, s);
     k_resid32<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, L.r);
     Level &C = ps->lev[l + 1];
     k_restrict<<<grid_for(C.n, nrhs), PT, 0, s>>>(L.nx, L.ny, L.fixed, L.r, C.nx, C.ny, C.b);
     vcycle(ps, l + 1, nrhs, s);
     k_prolong<<<g, PT, 0, s>>>(L.nx, L.ny, L.fixed, L.x, C.nx, C.ny, C.x);
-    for (int k = 0; k < ps->post; ++k) {
-        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 1);
-        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, 0);
-    }
+    for (int k = 0; k < ps->post; ++k) sweep(L, nrhs, false, s);
 }
 
 // z = M r : copies r into the level-0 right-hand side, runs the V-cycle, copies x out.
@@ -357,6 +373,7 @@ void tb_poisson_free(tb_poisson *ps) {
     cudaFree(ps->d64); cudaFree(ps->ke64); cudaFree(ps->kn64); cudaFree(ps->r64);
     cudaFree(ps->e); cudaFree(ps->pr); cudaFree(ps->pz); cudaFree(ps->pp); cudaFree(ps->pq);
     cudaFree(ps->scal);
+    cudaFree(ps->part);
     delete ps;
 }
 
@@ -421,7 +438,8 @@ extern "C" int tb_poisson_setup(tb_ctx *ctx, const double *h_diag, const double 
     if ((rc = upload<double>(ctx, &ps->r64, nullptr, vec)) || (rc = upload<float>(ctx, &ps->e, nullptr, vec)) ||
         (rc = upload<float>(ctx, &ps->pr, nullptr, vec)) || (rc = upload<float>(ctx, &ps->pz, nullptr, vec)) ||
         (rc = upload<float>(ctx, &ps->pp, nullptr, vec)) || (rc = upload<float>(ctx, &ps->pq, nullptr, vec)) ||
-        (rc = upload<double>(ctx, &ps->scal, nullptr, (size_t)max_rhs * 8))) {
+        (rc = upload<double>(ctx, &ps->scal, nullptr, (size_t)max_rhs * 8)) ||
+        (rc = upload<double>(ctx, &ps->part, nullptr, (size_t)max_rhs * ((n + PT - 1) / PT) * 2))) {
         tb_poisson_free(ps);
         return rc;
     }
@@ -452,7 +470,8 @@ extern "C" int tb_poisson_solve(tb_ctx *ctx, int nrhs, const double *d_b, double
     double worst = 0;
     for (;;) {
         k_clear_slots<<<sb, PT, 0, s>>>(nrhs, ps->scal, 0, 8);
-        k_resid64<<<g, PT, 0, s>>>(F.nx, F.ny, ps->d64, ps->ke64, ps->kn64, d_x, d_b, ps->r64, ps->scal);
+        k_resid64<<<g, PT, 0, s>>>(F.nx, F.ny, ps->d64, ps->ke64, ps->kn64, d_x, d_b, ps->r64, ps->part);
+        k_sum_partials<<<(2 * nrhs + PT - 1) / PT, PT, 0, s>>>(nrhs, g.x, 2, ps->part, ps->scal, S_RR);
         TB_CUDA(ctx, cudaMemcpyAsync(sc.data(), ps->scal, sc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
         TB_CUDA(ctx, cudaStreamSynchronize(s));
         worst = 0;
@@ -469,10 +488,12 @@ extern "C" int tb_poisson_solve(tb_ctx *ctx, int nrhs, const double *d_b, double
         k_normalise<<<g, PT, 0, s>>>(n, ps->r64, ps->pr, ps->e, ps->scal);
         for (int it = 0; it < inner; ++it) {
             precondition(ps, nrhs, ps->pr, ps->pz, s);
-            k_dot<<<g, PT, 0, s>>>(n, ps->pr, ps->pz, ps->scal, S_RZ_NEW);
+            k_dot<<<g, PT, 0, s>>>(n, ps->pr, ps->pz, ps->part);
+            k_sum_partials<<<(nrhs + PT - 1) / PT, PT, 0, s>>>(nrhs, g.x, 1, ps->part, ps->scal, S_RZ_NEW);
             k_update_p<<<g, PT, 0, s>>>(n, ps->pz, ps->pp, ps->scal, it == 0);
             k_shift_rz<<<sb, PT, 0, s>>>(nrhs, ps->scal);
-            k_matvec_dot<<<g, PT, 0, s>>>(F.nx, F.ny, F.d, F.ke, F.kn, F.fixed, ps->pp, ps->pq, ps->scal);
+            k_matvec_dot<<<g, PT, 0, s>>>(F.nx, F.ny, F.d, F.ke, F.kn, F.fixed, ps->pp, ps->pq, ps->part);
+            k_sum_partials<<<(nrhs + PT - 1) / PT, PT, 0, s>>>(nrhs, g.x, 1, ps->part, ps->scal, S_PQ);
             k_axpy<<<g, PT, 0, s>>>(n, ps->pp, ps->pq, ps->e, ps->pr, ps->scal);
         }
         k_correct<<<g, PT, 0, s>>>(n, ps->e, d_x, ps->scal);

@@ -21,6 +21,9 @@
 // trench_trace.cu:92-148): vacuum-weighted bilinear field, CFL step, trapezoid
 // update, periodic x, escape at the top, staircase corner crossing, first-face
 // wall entry and the potential-barrier reflection.
+#include <algorithm>
+#include <vector>
+
 #include "tb_internal.cuh"
 
 namespace {
@@ -68,9 +71,10 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 // Bulk-copies `bytes` (multiple of 16) from global to shared memory through the
 // async copy engine and waits on an mbarrier with a bounded number of polls.
 // Returns false if the copy did not complete within the bound.
-__device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mbar) {
+__device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mbar, bool reuse = false) {
     const uint32_t bar = smem_u32(mbar);
     if (threadIdx.x == 0) {
+        if (reuse) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -96,27 +100,24 @@ __device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mba
     return __syncthreads_and(done) != 0;
 }
 
+// Traces particles of one case with the calling warp until the case's queue is
+// drained and every lane of the warp is empty, then adds the warp's tallies to the
+// case's totals.  `fieldp` is the packed field in shared or global memory.
 template <bool SMEM>
-__global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t mbar;
+__device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const tb_trace_args &a = k.a;
     const int nx = k.nx, ny = k.ny;
     const int cells = nx * ny;
     const int P = ny + 2;  // padded column stride
+    const float inv_v = k.inv_v;
+    const float4 *const barrier_tab = k.barrier;
+    int *const err = k.err;
+    unsigned long long *const queue = k.queue;
 
     FieldView<SMEM> F;
-    if (SMEM) {
-        if (!stage_field(smem_raw, k.field, k.bytes, &mbar)) {
-            if (threadIdx.x == 0) atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BULK_TIMEOUT);
-            return;
-        }
-        F.p = reinterpret_cast<const tb_fcell *>(smem_raw);
-    } else {
-        F.p = k.field;
-    }
+    F.p = fieldp;
 
     const float cfl = (float)a.cfl;
     const bool barrier = a.d_phi != nullptr;
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
                 const int leader = __ffs(need) - 1;
                 const int cnt = __popc(need);
                 unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(k.queue, (unsigned long long)cnt);
+                if (lane == leader) base = atomicAdd(queue, (unsigned long long)cnt);
                 base = __shfl_sync(FULL, base, leader);
                 if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
                 if (pid < 0) {
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
         const float speed = sqrtf(vx * vx + vy * vy);
         const float acc = sqrtf(ax * ax + ay * ay);
-        const float dt = __fdividef(cfl, speed + sqrtf(2.f * acc) + k.inv_v);
+        const float dt = __fdividef(cfl, speed + sqrtf(2.f * acc) + inv_v);
         const float vxn = vx + ax * dt, vyn = vy + ay * dt;
         const float sx = 0.5f * (vx + vxn) * dt, sy = 0.5f * (vy + vyn) * dt;
         float nox = ox + sx, noy = oy + sy;
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
             hit = !F.vac((cx + 1) * P + cy + 1);
             dcell = ccell;
             if (hit && barrier) {
-                const float4 b = __ldg(k.barrier + ccell);
+                const float4 b = __ldg(barrier_tab + ccell);
                 // neighbour the particle came from: W/E across an x face, S/N across a y face
                 const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
                 const float vn = face_x ? vxn : vyn;
@@ -260,7 +261,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         int done = 0;
         if (hit) {
             if (dcell < 0 || dcell >= cells) {
-                atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BAD_CELL);
+                atomicCAS(err, TB_DERR_NONE, TB_DERR_BAD_CELL);
             } else {
                 atomicAdd(a.d_counts + (size_t)spc * cells + dcell, 1);
             }
@@ -304,6 +305,69 @@ __global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_
         if (my_steps) atomicAdd(t + 3, (unsigned long long)my_steps);
         if (my_hit_i) atomicAdd(t + 4, (unsigned long long)my_hit_i);
         if (my_hit_e) atomicAdd(t + 5, (unsigned long long)my_hit_e);
+    }
+}
+
+template <bool SMEM>
+__global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    const tb_fcell *fieldp = k.field;
+    if (SMEM) {
+        if (!stage_field(smem_raw, k.field, k.bytes, &mbar)) {
+            if (threadIdx.x == 0) atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BULK_TIMEOUT);
+            return;
+        }
+        fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
+    }
+    run_case<SMEM>(k, fieldp);
+}
+
+// Many cases in one persistent launch: each CTA repeatedly takes the case with the
+// most particles left in its queue, stages that case's field into shared memory and
+// traces from the case's queue; CTAs meet on large cases and spread over small ones.
+template <bool SMEM>
+__global__ void __launch_bounds__(F32_THREADS, 1)
+    trace_f32_batch_kernel(const K32 *__restrict__ cases, int n_cases, int *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ int s_case;
+    bool staged = false;
+    for (;;) {
+        if (threadIdx.x < 32) {
+            // warp 0: the case with the most unclaimed particles
+            long long best_rem = 0;
+            int best = -1;
+            for (int c = threadIdx.x; c < n_cases; c += 32) {
+                const unsigned long long q = *reinterpret_cast<volatile const unsigned long long *>(cases[c].queue);
+                const long long rem = cases[c].a.n - (long long)q;
+                if (rem > best_rem) { best_rem = rem; best = c; }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const long long r2 = __shfl_down_sync(0xffffffffu, best_rem, o);
+                const int b2 = __shfl_down_sync(0xffffffffu, best, o);
+                if (r2 > best_rem || (r2 == best_rem && b2 >= 0 && (best < 0 || b2 < best))) {
+                    best_rem = r2;
+                    best = b2;
+                }
+            }
+            if (threadIdx.x == 0) s_case = best;
+        }
+        __syncthreads();
+        const int c = s_case;
+        if (c < 0) return;
+        const K32 &k = cases[c];
+        const tb_fcell *fieldp = k.field;
+        if (SMEM) {
+            if (!stage_field(smem_raw, k.field, k.bytes, &mbar, staged)) {
+                if (threadIdx.x == 0) atomicCAS(err, TB_DERR_NONE, TB_DERR_BULK_TIMEOUT);
+                return;
+            }
+            staged = true;
+            fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
+        }
+        run_case<SMEM>(k, fieldp);
+        __syncthreads();  // every warp is done with this case's field
     }
 }
 
@@ -352,9 +416,33 @@ int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const
 int tb_configure_trace_f32(tb_ctx *ctx) {
     const int limit = ctx->max_smem - 1024;
     TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      limit));
     ctx->smem_attr_bytes = limit;
     return TB_OK;
 }
+
+namespace {
+
+K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
+    K32 k;
+    k.a = *a;
+    k.nx = ctx->nx;
+    k.ny = ctx->ny;
+    k.dx = ctx->dx;
+    k.vscale = ctx->vscale;
+    k.inv_v = (float)(1.0 / ctx->vscale);
+    k.inv_dx = 1.0 / ctx->dx;
+    k.inv_v64 = 1.0 / ctx->vscale;
+    k.field = ctx->d_field;
+    k.barrier = ctx->d_barrier;
+    k.queue = ctx->d_queue;
+    k.err = ctx->d_err;
+    k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
+    return k;
+}
+
+}  // namespace
 
 int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     K32 k;
@@ -480,5 +568,152 @@ extern "C" int tb_trace_f32_noalloc(int nx, int ny, double dx, const uint8_t *d_
     e = cudaMemsetAsync(a->d_totals + 6, 0, sizeof(int64_t), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(a->d_totals + 6, tmp.d_err, sizeof(int), cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "copy of the check flag");
+    return TB_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// Case packs: many trench cases traced by one persistent launch.
+
+struct tb_pack {
+    int device = 0;
+    int n = 0;
+    std::vector<tb_ctx *> ctxs;
+    K32 *d_cases = nullptr;
+    unsigned long long *d_queues = nullptr;  // one work counter per case
+    int *d_err = nullptr;
+    int max_bytes = 0;
+    int max_particles = 0;
+    bool smem = false;
+    int num_sms = 0;
+    int ready = 0;
+    char err[512] = {0};
+};
+
+namespace {
+
+// status = live, steps = 0, counts = 0, totals = 0 for every case (blockIdx.y = case)
+__global__ void k_pack_reset(const K32 *cases, int n_cases) {
+    const int c = blockIdx.y;
+    if (c >= n_cases) return;
+    const K32 &k = cases[c];
+    const long long n = k.a.n;
+    const int cells2 = 2 * k.nx * k.ny;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n || i < cells2;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < n) { k.a.d_status[i] = 3; k.a.d_steps[i] = 0; }
+        if (i < cells2) k.a.d_counts[i] = 0;
+        if (i < 8) k.a.d_totals[i] = 0;
+    }
+}
+
+}  // namespace
+
+static int pack_fail(tb_pack *p, int code, const char *msg) {
+    if (p) snprintf(p->err, sizeof(p->err), "%s", msg);
+    return tb_fail(nullptr, code, "%s", msg);
+}
+
+extern "C" int tb_pack_create(tb_pack **out, int n_cases, tb_ctx *const *ctxs) {
+    if (!out || n_cases < 1 || !ctxs) return tb_fail(nullptr, TB_ERR_ARG, "tb_pack_create: no cases");
+    *out = nullptr;
+    const int dev = ctxs[0] ? ctxs[0]->device : -1;
+    for (int i = 0; i < n_cases; ++i)
+        if (!ctxs[i] || ctxs[i]->device != dev)
+            return tb_fail(nullptr, TB_ERR_ARG, "tb_pack_create: every case needs a context on the same device");
+    tb_pack *p = new tb_pack();
+    p->device = dev;
+    p->n = n_cases;
+    p->ctxs.assign(ctxs, ctxs + n_cases);
+    p->num_sms = ctxs[0]->num_sms;
+    for (int i = 0; i < n_cases; ++i)
+        p->max_bytes = std::max(p->max_bytes, tb_halo_count(ctxs[i]->nx, ctxs[i]->ny) * (int)sizeof(tb_fcell));
+    p->smem = p->max_bytes <= ctxs[0]->smem_attr_bytes;
+    cudaError_t e = cudaSetDevice(dev);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_cases, sizeof(K32) * n_cases);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_queues, sizeof(unsigned long long) * n_cases);
+    if (e == cudaSuccess) e = cudaMalloc(&p->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(p->d_err, 0, sizeof(int));
+    if (e != cudaSuccess) {
+        cudaFree(p->d_cases); cudaFree(p->d_queues); cudaFree(p->d_err);
+        delete p;
+        return tb_cuda_check(nullptr, e, "tb_pack_create");
+    }
+    *out = p;
+    return TB_OK;
+}
+
+extern "C" int tb_pack_destroy(tb_pack *p) {
+    if (!p) return TB_OK;
+    cudaSetDevice(p->device);
+    cudaFree(p->d_cases);
+    cudaFree(p->d_queues);
+    cudaFree(p->d_err);
+    delete p;
+    return TB_OK;
+}
+
+extern "C" const char *tb_pack_last_error(const tb_pack *p) { return p ? p->err : tb_last_error(nullptr); }
+
+extern "C" int tb_pack_set_args(tb_pack *p, const tb_trace_args *args) {
+    if (!p || !args) return TB_ERR_ARG;
+    std::vector<K32> ks(p->n);
+    p->max_particles = 0;
+    for (int i = 0; i < p->n; ++i) {
+        const tb_trace_args &a = args[i];
+        if (a.n < 0 || a.n > 0x7fffffffLL || !(a.cfl > 0 && a.cfl <= 1) || a.max_steps < 1 || a.step_budget < 1)
+            return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: invalid particle count, cfl or step counts");
+        if (a.n_phase > 0 || a.record)
+            return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: the case pack traces in FP32 without RF or record");
+        if (!a.d_x || !a.d_y || !a.d_vx || !a.d_vy || !a.d_qm || !a.d_spc || !a.d_counts || !a.d_totals ||
+            !a.d_status || !a.d_steps)
+            return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: a required array is missing");
+        if ((a.d_phi == nullptr) != (a.d_wface == nullptr))
+            return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: phi and wface must be given together");
+        if (!p->ctxs[i]->fields_ready)
+            return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: a case has no packed field yet");
+        ks[i] = make_k32(p->ctxs[i], &a);
+        ks[i].queue = p->d_queues + i;
+        ks[i].err = p->d_err;
+        p->max_particles = std::max<int>(p->max_particles, (int)a.n);
+    }
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e == cudaSuccess) e = cudaMemcpy(p->d_cases, ks.data(), sizeof(K32) * p->n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
+    p->ready = 1;
+    return TB_OK;
+}
+
+extern "C" int tb_pack_trace(tb_pack *p, int reset, void *stream) {
+    if (!p) return TB_ERR_ARG;
+    if (!p->ready) return pack_fail(p, TB_ERR_ARG, "tb_pack_trace: call tb_pack_set_args first");
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e == cudaSuccess) e = cudaMemsetAsync(p->d_queues, 0, sizeof(unsigned long long) * p->n, s);
+    if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
+    if (reset) {
+        const int blocks = std::max(1, std::min(64, (p->max_particles + 255) / 256));
+        k_pack_reset<<<dim3(blocks, p->n), 256, 0, s>>>(p->d_cases, p->n);
+    }
+    if (p->smem)
+        trace_f32_batch_kernel<true><<<p->num_sms, F32_THREADS, p->max_bytes, s>>>(p->d_cases, p->n, p->d_err);
+    else
+        trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, 0, s>>>(p->d_cases, p->n, p->d_err);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
+    return TB_OK;
+}
+
+extern "C" int tb_pack_check(tb_pack *p, void *stream) {
+    if (!p) return TB_ERR_ARG;
+    int flag = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
+    if (flag != TB_DERR_NONE) {
+        cudaMemsetAsync(p->d_err, 0, sizeof(int), s);
+        return pack_fail(p, TB_ERR_KERNEL, "a kernel check failed in the case pack");
+    }
     return TB_OK;
 }

@@ -76,6 +76,31 @@ def boundary_rhs(p, eps, volts, fixed_sides=True):
     return rhs
 
 
+def _grad(c, m, pl, vm, vp, dx):
+    """trench_charging_2d.py:429-436"""
+    g = np.zeros_like(c)
+    g = np.where(vm & vp, (pl - m) / (2 * dx), g)
+    g = np.where(vp & ~vm, (pl - c) / dx, g)
+    g = np.where(vm & ~vp, (c - m) / dx, g)
+    return -g
+
+
+def compute_field(phi, vac, p, top_voltage=None):
+    """E = -grad phi over vacuum neighbours, host version for setup (trench_charging_2d.py:439-454);
+    the per-batch field is computed on the device (tb_step_potential)."""
+    dx = p.dx
+    ex = _grad(phi, np.roll(phi, 1, 0), np.roll(phi, -1, 0), np.roll(vac, 1, 0), np.roll(vac, -1, 0), dx)
+    vtop = p.top_voltage if top_voltage is None else top_voltage
+    ghost_top = 2 * vtop - phi[:, -1] if p.top_bc == "dirichlet" else phi[:, -1]
+    ghost_bot = 2 * p.substrate_voltage - phi[:, 0]
+    pd = np.concatenate([ghost_bot[:, None], phi[:, :-1]], axis=1)
+    pu = np.concatenate([phi[:, 1:], ghost_top[:, None]], axis=1)
+    f = np.zeros((phi.shape[0], 1), dtype=bool)
+    vd = np.concatenate([f, vac[:, :-1]], axis=1)
+    vu = np.concatenate([vac[:, 1:], ~f], axis=1)
+    return ex, _grad(phi, pd, pu, vd, vu, dx)
+
+
 def circuit_voltages(c, phase):
     """Periodic interpolation of the circuit potentials (trench_charging_2d.py:312-320)."""
     t = np.asarray(c["t"])
@@ -107,6 +132,15 @@ def field_voltages(p, mask, circuit=None):
     if p.field_mode == "circuit":
         return circuit_voltages(circuit, p.rf_phase)
     if p.field_mode == "circuit_rf":
+        if not isinstance(p.rf_time_steps, (int, np.integer)) or p.rf_time_steps < 16:
+            raise ValueError("rf_time_steps must be an integer >= 16")
+        t = np.asarray(circuit["t"])
+        period = (t[1] - t[0]) * t.size
+        if (not np.isfinite(period) or period <= 0 or not np.isclose(t[0], 0, atol=period * 1e-12)
+                or not np.allclose(np.diff(t), period / t.size, rtol=1e-10, atol=period * 1e-12)):
+            raise ValueError("the circuit waveform must be one period sampled evenly from t = 0")
+        if not np.isfinite(p.dt_batch) or p.dt_batch < period * (1 - 1e-12):
+            raise ValueError("circuit_rf needs dt_batch of at least one RF period")
         wave = np.column_stack((circuit["uw"] - circuit["up"], circuit["um"] - circuit["up"]))
         mean = wave.mean(axis=0)
         return dict(substrate=float(mean[0]), mask=float(mean[1]), top=0.0, sheath=float(np.mean(circuit["V1"])))

@@ -88,3 +88,10 @@ def mixture_energy(components):
                 raise ValueError(f"unknown energy component {kind!r}")
         return out
     return sample
+
+
+def launch_times(rng, n, period):
+    """Stratified RF launch times over one period, shuffled (trench_rf.py:14-18)."""
+    times = (np.arange(n) + rng.random(n)) * period / n
+    rng.shuffle(times)
+    return times

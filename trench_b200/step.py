@@ -19,8 +19,8 @@ import numpy as np
 import torch
 
 from . import _capi, geometry
-from .fields import FieldSolver, apply_matrix, boundary_rhs, field_voltages
-from .inject import inject
+from .fields import FieldSolver, apply_matrix, boundary_rhs, compute_field, field_voltages
+from .inject import inject, launch_times
 from .params import E_CHARGE, EPS0, WALL_MODELS, is_tapered
 from .tracer import DEFAULT_VSCALE, Context, _ptr
 
@@ -36,9 +36,6 @@ class ChargingCase:
             raise ValueError("green must be f32 or f64")
         if p.wall_model not in WALL_MODELS:
             raise ValueError(f"wall_model must be one of {WALL_MODELS}: {p.wall_model!r}")
-        if p.field_mode == "circuit_rf":
-            raise ValueError("field_mode circuit_rf is traced by B200Tracer(rf=...); the device batch loop "
-                             "covers floating / fixed / circuit")
         if not (0 < p.cfl <= 1) or p.max_steps < 1:
             raise ValueError("CUDA tracing needs 0 < cfl <= 1 and max_steps >= 1")
         if not torch.cuda.is_available():
@@ -150,6 +147,9 @@ class ChargingCase:
             self._args = _capi.TraceArgs()
             self._graph = None
             self.trace_events = None   # optional (start, end) CUDA events around the tracer launch
+            self.rf = None
+            if p.field_mode == "circuit_rf":
+                self._build_rf(circuit, solver, eps, cond, vac)
             # initial field (trench_charging_2d.py:1198)
             self._potential()
 
@@ -173,6 +173,34 @@ class ChargingCase:
         self.G = G.contiguous()
         self.P = P
         self.green = green
+
+    def _build_rf(self, circuit, solver, eps, cond, vac):
+        """Unit-voltage basis of the electrodes and the period-resolved voltage deltas
+        (trench_charging_2d.py:397-412); the tracer superposes them in flight."""
+        p, dev, nx, ny = self.p, self.dev, self.nx, self.ny
+        t = np.asarray(circuit["t"])
+        period = (t[1] - t[0]) * t.size
+        wave = np.column_stack((circuit["uw"] - circuit["up"], circuit["um"] - circuit["up"]))
+        mean = wave.mean(axis=0)
+        basis = []
+        for vs, vm in ((1.0, 0.0), (0.0, 1.0)):
+            brhs = boundary_rhs(p, eps, dict(substrate=vs, mask=vm, top=0.0), fixed_sides=False)
+            bc = cond.astype(float) * vm
+            b = brhs - apply_matrix(solver.diag, solver.ce, solver.cn, bc)
+            basis.append((solver.solve(b.ravel()) + bc.ravel()).reshape(nx, ny))
+        basis = np.array(basis)
+        electric = [compute_field(v, vac, p, 0.0) for v in basis]
+        dt_max = period / p.rf_time_steps
+        if p.rf_wave == "pulse":
+            dt_max = min(dt_max, p.rf_rise / 8)
+        w = wave - mean
+        self.rf = dict(period=float(period), wave=w, phi=basis, Ex=np.array([e[0] for e in electric]),
+                       Ey=np.array([e[1] for e in electric]), dt_max=float(dt_max))
+        f = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+        self.t_rf = dict(ex=f(self.rf["Ex"]), ey=f(self.rf["Ey"]), phi=f(basis), wave=f(w))
+        bound = np.abs(w).max(axis=0)
+        self.rf_bound = (float(bound[0]), float(bound[1]))
+        self.clock = torch.zeros((self.capacity, 2), dtype=torch.float64, device=dev)
 
     def _leak_graph(self, sx, sy):
         """Conductance graph of the surface cells (trench_charging_2d.py:778-792)."""
@@ -228,9 +256,15 @@ class ChargingCase:
         self.ctx.check(_capi.lib().tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), self._stream()))
 
     # ---- per batch -----------------------------------------------------------------
-    def load(self, x, y, vx, vy, qm, spc, non_blocking=False):
-        """Copy one batch of injected particles into the device buffers."""
+    def load(self, x, y, vx, vy, qm, spc, non_blocking=False, launch_times=None):
+        """Copy one batch of injected particles into the device buffers (with their RF
+        launch times in circuit_rf mode)."""
         n = len(x)
+        if self.rf is not None:
+            if launch_times is None or len(launch_times) != n:
+                raise ValueError("circuit_rf needs one launch time per particle")
+            t0 = np.asarray(launch_times, dtype=np.float64) % self.rf["period"]
+            self.clock[:n].copy_(torch.from_numpy(np.column_stack((t0, np.zeros(n)))), non_blocking=False)
         if n > self.capacity:
             raise ValueError(f"{n} particles exceed the case capacity {self.capacity}")
         if any(len(v) != n for v in (y, vx, vy, qm, spc)):
@@ -266,11 +300,21 @@ class ChargingCase:
         a.d_status, a.d_steps = _ptr(self.status), _ptr(self.steps)
         a.d_hit = None
         a.write_state = 0
+        precision = self.precision
+        if self.rf is not None:
+            # the in-flight RF clock runs on the FP64 kernel
+            precision = "f64"
+            a.d_rf_ex, a.d_rf_ey, a.d_rf_phi = _ptr(self.t_rf["ex"]), _ptr(self.t_rf["ey"]), _ptr(self.t_rf["phi"])
+            a.d_wave = _ptr(self.t_rf["wave"])
+            a.n_phase = len(self.rf["wave"])
+            a.period, a.dt_max = self.rf["period"], self.rf["dt_max"]
+            a.bound_vs, a.bound_vm = self.rf_bound
+            a.d_clock = _ptr(self.clock)
         ev = getattr(self, "trace_events", None)
         if ev is not None:
             ev[0].record()
         if n:
-            self.ctx.check(L.tb_trace(self.ctx.handle, ctypes.byref(a), _capi.PRECISION[self.precision], s))
+            self.ctx.check(L.tb_trace(self.ctx.handle, ctypes.byref(a), _capi.PRECISION[precision], s))
         if ev is not None:
             ev[1].record()
         self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
@@ -327,9 +371,19 @@ class ChargingCase:
         p = self.p
         n_batches = p.n_batches if n_batches is None else n_batches
         rng = np.random.default_rng(p.seed) if rng is None else rng
+        if p.field_mode in ("circuit", "circuit_rf") and ion_energy is None and ion_velocity is None:
+            # ions start at the plasma potential with the Bohm energy (trench_charging_2d.py:1135-1139)
+            ion_energy = lambda r, k: np.full(k, p.electron_temp_eV / 2)
+        phase_rng = (np.random.default_rng(np.random.SeedSequence([p.seed, 0x5246]))
+                     if self.rf is not None else None)
         with torch.cuda.device(self.dev):
             for b in range(n_batches):
-                self.load(*inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity))
+                parts = inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity)
+                t0 = None
+                if phase_rng is not None:
+                    t0 = np.concatenate([launch_times(phase_rng, p.n_per_batch, self.rf["period"])
+                                         for _ in range(2)])
+                self.load(*parts, launch_times=t0)
                 self.step()
                 if log is not None and ((b + 1) % 10 == 0 or b == 0):
                     log(f"[{b + 1}/{n_batches}]")
