@@ -288,6 +288,8 @@ def run_b200(args, p):
         flush.zero_()
         s1.synchronize()
         e2e_ms.append(s0.elapsed_time(s1))
+    # device injection: the batch is drawn on the GPU (Philox) inside the captured graph
+    dinj = device_injection(case, p, args.steps)
     clk = clocks.stop()
     case.check()
     h2d = sum(t.numel() * t.element_size() for t in host[0])
@@ -334,6 +336,7 @@ def run_b200(args, p):
             "e2e": {"value": particles / (e2e_total / 1000.0), "unit": "particles/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "batches_per_s": 1000.0 * args.steps * world / e2e_total},
+            "device_injection": dinj,
             "gpu_launches": 10 * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "wall_s": wall}
@@ -392,6 +395,44 @@ def run_sweep(args):
             "batches_per_s": 1000.0 / float(np.mean(ms)), "particle_steps_per_batch": float(steps_per_batch)}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def device_injection(case, p, steps):
+    """Particles/s when each batch is also injected on the device (tb_inject inside the
+    captured graph: bimodal IED and half-Gaussian IAD tables, Maxwellian electrons)."""
+    import torch
+    from trench_b200 import inject
+    et = inject.table_from_pdf(inject.bimodal_gaussian_pdf(40.0, 6.0, 140.0, 6.0), 0.0, 200.0)
+    at = inject.table_from_pdf(inject.half_gaussian_pdf(np.radians(3.0)), 0.0, np.radians(18.0))
+    inj = inject.DeviceInjector(case, seed=2024, energy_table=et, angle_table=at)
+    n = 2 * p.n_per_batch
+    side = torch.cuda.Stream(case.dev)
+    side.wait_stream(torch.cuda.current_stream(case.dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(side):
+        with torch.cuda.graph(g, stream=side):
+            inj()
+            case.step(n)
+    torch.cuda.current_stream(case.dev).wait_stream(side)
+    g.replay()
+    torch.cuda.synchronize()
+    ms = []
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=case.dev)
+    row = torch.empty(case.hist_cols, dtype=torch.float64).pin_memory()
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        row.copy_(case.hist[min(case.batches_done() - 1, case.max_batches - 1)], non_blocking=True)
+        e1.record()
+        flush.zero_()
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    del g
+    return {"value": n / (float(np.mean(ms)) / 1000.0), "unit": "particles/s", "ms_per_step": float(np.mean(ms)),
+            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": row.numel() * row.element_size(),
+            "note": "inject (Philox, tabulated IED/IAD) + batch step replayed from one CUDA graph; "
+                    "history row read back each step"}
 
 
 def case_smem_peak(case):

@@ -170,6 +170,40 @@ int tb_step_charge(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
  * tb_set_fields) and probe history. */
 int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
 
+/* ---- Device-side injection -------------------------------------------------------
+ * Samples n_species ions (indices [0, n)) then n_species electrons ([n, 2n)) into the
+ * particle arrays, restating the reference's `inject` (trench_charging_2d.py:458-489)
+ * on the GPU.  Random numbers: Philox4x32-10, counter (i, batch) and key seed, so the
+ * draws do not depend on the launch.  Ion energy (eV) and polar angle (rad) come from
+ * histogram tables (bin edges and cumulative weights, n + 1 entries each, sampled
+ * linearly within a bin); n_energy = 0 uses ion_energy_eV, n_angle = 0 a lateral
+ * thermal velocity N(0, ion_lateral_sigma).  No counterpart in the reference, which
+ * samples on the host with NumPy. */
+typedef struct {
+    int64_t n_species;
+    uint64_t seed, batch;
+    double *d_x, *d_y, *d_vx, *d_vy, *d_qm;
+    int8_t *d_spc;
+    double lx, y0;                   /* domain width and injection height, metres */
+    double qm_ion, qm_electron;      /* C/kg */
+    double ion_mass, e_charge;       /* kg, C */
+    double electron_sigma;           /* sqrt(Te e / m_e), m/s */
+    double ion_energy_eV, ion_lateral_sigma;
+    const double *d_energy_edges, *d_energy_cdf;
+    int n_energy;                    /* bins of the energy table, 0 = fixed energy */
+    const double *d_angle_edges, *d_angle_cdf;
+    int n_angle;                     /* bins of the angle table, 0 = lateral thermal */
+    int angle_random_sign;           /* draw the sign of the angle with probability 1/2 */
+    const int32_t *d_counter;        /* optional device batch counter: the Philox batch word is
+                                        batch + *d_counter + 1 (lets a CUDA graph replay a new batch) */
+} tb_inject_args;
+
+int tb_inject(tb_ctx *ctx, const tb_inject_args *args, void *stream);
+/* The raw Philox4x32-10 stream: 4 words per index i < n for counter (i, batch) and
+ * key seed, into d_out (4n words).  For checking the generator. */
+int tb_philox_fill(tb_ctx *ctx, unsigned long long seed, unsigned long long batch, int n, uint32_t *d_out,
+                   void *stream);
+
 /* ---- Case packs: many trench cases in one persistent FP32 launch -----------------
  * A pack groups contexts of one device (different grids allowed).  tb_pack_set_args
  * takes one tb_trace_args per case (FP32 rules of tb_trace; the cases' fields must

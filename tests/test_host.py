@@ -88,3 +88,28 @@ def test_sweep_cases_are_valid_and_spread():
     kinds = {p.mask_type for p in ps}
     assert kinds == {"conductor", "dielectric"}
     assert 30 <= min(seps) and max(seps) <= 150
+
+
+def test_philox_known_answer_vectors():
+    """Philox4x32-10 known-answer vectors of the published Random123 test set."""
+    from trench_b200.inject import philox4x32_10
+    kat = [((0, 0, 0, 0), (0, 0), (0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8)),
+           ((0xffffffff,) * 4, (0xffffffff, 0xffffffff), (0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd)),
+           ((0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344), (0xa4093822, 0x299f31d0),
+            (0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1))]
+    for c, k, want in kat:
+        assert tuple(int(v) for v in philox4x32_10([c], k)[0]) == want
+
+
+def test_histogram_tables():
+    from trench_b200.inject import bimodal_gaussian_pdf, histogram_table, table_from_pdf
+    e, c = histogram_table([0, 1, 2, 4], [1, 0, 3])
+    np.testing.assert_allclose(c, [0, 0.25, 0.25, 1.0])
+    with pytest.raises(ValueError):
+        histogram_table([0, 1, 1], [1, 1])
+    with pytest.raises(ValueError):
+        histogram_table([0, 1, 2], [0, 0])
+    e, c = table_from_pdf(bimodal_gaussian_pdf(40, 6, 140, 6), 0, 200)
+    assert c[0] == 0 and c[-1] == 1 and np.all(np.diff(c) >= 0)
+    # the median of the symmetric bimodal density lies between the peaks
+    assert 60 < np.interp(0.5, c, e) < 120

@@ -74,6 +74,27 @@ class StepDesc(ctypes.Structure):
     ]
 
 
+class InjectArgs(ctypes.Structure):
+    """Mirror of ``tb_inject_args``."""
+    _fields_ = [
+        ("n_species", _i64),
+        ("seed", ctypes.c_uint64), ("batch", ctypes.c_uint64),
+        ("d_x", _vp), ("d_y", _vp), ("d_vx", _vp), ("d_vy", _vp), ("d_qm", _vp),
+        ("d_spc", _vp),
+        ("lx", _dbl), ("y0", _dbl),
+        ("qm_ion", _dbl), ("qm_electron", _dbl),
+        ("ion_mass", _dbl), ("e_charge", _dbl),
+        ("electron_sigma", _dbl),
+        ("ion_energy_eV", _dbl), ("ion_lateral_sigma", _dbl),
+        ("d_energy_edges", _vp), ("d_energy_cdf", _vp),
+        ("n_energy", ctypes.c_int),
+        ("d_angle_edges", _vp), ("d_angle_cdf", _vp),
+        ("n_angle", ctypes.c_int),
+        ("angle_random_sign", ctypes.c_int),
+        ("d_counter", _vp),
+    ]
+
+
 SFLAG_COND, SFLAG_REGION, SFLAG_BOTTOM = 1, 2, 4
 
 # Every symbol the header declares, with its ctypes signature.
@@ -93,6 +114,8 @@ SIGNATURES = {
     "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
+    "tb_inject": (ctypes.c_int, [_vp, ctypes.POINTER(InjectArgs), _vp]),
+    "tb_philox_fill": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int, _vp, _vp]),
     "tb_pack_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
     "tb_pack_destroy": (ctypes.c_int, [_vp]),
     "tb_pack_last_error": (ctypes.c_char_p, [_vp]),

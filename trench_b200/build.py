@@ -25,6 +25,7 @@ UNITS = {
     "tb_poisson.cu": [],
     "tb_step.cu": ["-fmad=false"],
     "tb_bench.cu": [],
+    "tb_inject.cu": [],
 }
 
 

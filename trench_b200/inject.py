@@ -95,3 +95,118 @@ def launch_times(rng, n, period):
     times = (np.arange(n) + rng.random(n)) * period / n
     rng.shuffle(times)
     return times
+
+
+# ---- device-side injection ---------------------------------------------------------
+
+def philox4x32_10(counters, key):
+    """Philox4x32-10 (Salmon et al., SC'11) on the host: counters (n, 4) uint32, key
+    (k0, k1) -> (n, 4) uint32.  The device generator of tb_inject computes the same."""
+    c = np.array(counters, dtype=np.uint64) & 0xFFFFFFFF
+    k0, k1 = np.uint64(key[0] & 0xFFFFFFFF), np.uint64(key[1] & 0xFFFFFFFF)
+    m0, m1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
+    w0, w1 = np.uint64(0x9E3779B9), np.uint64(0xBB67AE85)
+    mask = np.uint64(0xFFFFFFFF)
+    for r in range(10):
+        if r:
+            k0 = (k0 + w0) & mask
+            k1 = (k1 + w1) & mask
+        p0 = m0 * c[:, 0]
+        p1 = m1 * c[:, 2]
+        hi0, lo0 = p0 >> np.uint64(32), p0 & mask
+        hi1, lo1 = p1 >> np.uint64(32), p1 & mask
+        c = np.stack([hi1 ^ c[:, 1] ^ k0, lo1, hi0 ^ c[:, 3] ^ k1, lo0], axis=1)
+    return c.astype(np.uint32)
+
+
+def histogram_table(edges, weights):
+    """Inverse-CDF table (edges, cdf) of a histogram with non-negative bin weights."""
+    edges = np.asarray(edges, dtype=np.float64)
+    w = np.asarray(weights, dtype=np.float64)
+    if edges.ndim != 1 or len(edges) != len(w) + 1 or np.any(np.diff(edges) <= 0):
+        raise ValueError("a table needs increasing bin edges, one more than the weights")
+    if np.any(w < 0) or not np.isfinite(w).all() or w.sum() <= 0:
+        raise ValueError("bin weights must be finite, non-negative and not all zero")
+    cdf = np.concatenate([[0.0], np.cumsum(w) / w.sum()])
+    cdf[-1] = 1.0
+    return edges, cdf
+
+
+def table_from_pdf(pdf, lo, hi, bins=1024):
+    """Histogram table of a density on [lo, hi] (bin-centre values times width)."""
+    edges = np.linspace(lo, hi, bins + 1)
+    centres = 0.5 * (edges[:-1] + edges[1:])
+    return histogram_table(edges, np.maximum(pdf(centres), 0.0) * np.diff(edges))
+
+
+def bimodal_gaussian_pdf(m1, s1, m2, s2, w1=0.5):
+    g = lambda e, m, s: np.exp(-0.5 * ((e - m) / s) ** 2) / (s * np.sqrt(2 * np.pi))
+    return lambda e: w1 * g(e, m1, s1) + (1 - w1) * g(e, m2, s2)
+
+
+def half_gaussian_pdf(sigma):
+    return lambda t: np.exp(-0.5 * (t / sigma) ** 2)
+
+
+class DeviceInjector:
+    """Fills a ChargingCase's particle buffers on the GPU each batch (tb_inject).
+
+    energy_table / angle_table: (edges, cdf) from histogram_table or table_from_pdf
+    (energy in eV, angle in radians); None uses p.ion_energy_eV / the lateral
+    thermal velocity of p.ion_temp_eV like the reference."""
+
+    def __init__(self, case, seed=0, energy_table=None, angle_table=None, angle_random_sign=True):
+        import ctypes
+        import torch
+        from . import _capi
+        from .params import AMU, E_CHARGE, M_E
+        from .tracer import _ptr
+        p = case.p
+        self.case = case
+        dev = case.dev
+        f = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+        a = _capi.InjectArgs()
+        a.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        a.n_species = int(p.n_per_batch)
+        a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in case.X)
+        a.d_spc = _ptr(case.SPC)
+        a.lx = p.nx * p.dx
+        a.y0 = case.ny * p.dx - 1e-3 * p.dx
+        m_i = p.ion_mass_amu * AMU
+        a.qm_ion, a.qm_electron = E_CHARGE / m_i, -E_CHARGE / M_E
+        a.ion_mass, a.e_charge = m_i, E_CHARGE
+        a.electron_sigma = float(np.sqrt(p.electron_temp_eV * E_CHARGE / M_E))
+        a.ion_energy_eV = float(p.ion_energy_eV)
+        a.ion_lateral_sigma = float(np.sqrt(p.ion_temp_eV * E_CHARGE / m_i))
+        self._keep = []
+        if energy_table is not None:
+            e, c = (f(v) for v in energy_table)
+            self._keep += [e, c]
+            a.d_energy_edges, a.d_energy_cdf, a.n_energy = _ptr(e), _ptr(c), len(energy_table[0]) - 1
+        if angle_table is not None:
+            e, c = (f(v) for v in angle_table)
+            self._keep += [e, c]
+            a.d_angle_edges, a.d_angle_cdf, a.n_angle = _ptr(e), _ptr(c), len(angle_table[0]) - 1
+        a.angle_random_sign = int(bool(angle_random_sign))
+        self.args = a
+        self._ctypes = ctypes
+        self._capi = _capi
+
+    def __call__(self, batch=None):
+        """Inject on the current stream: batch number `batch` (the Philox counter), or
+        with batch=None the case's own device batch counter + 1, so a captured CUDA
+        graph draws a fresh batch on every replay."""
+        import torch
+        from .tracer import _ptr
+        case = self.case
+        if 2 * self.args.n_species > case.capacity:
+            raise ValueError("the case buffers hold fewer particles than one batch")
+        if batch is None:
+            self.args.batch = 0
+            self.args.d_counter = _ptr(case.batch)
+        else:
+            self.args.batch = int(batch)
+            self.args.d_counter = None
+        s = self._ctypes.c_void_p(torch.cuda.current_stream(case.dev).cuda_stream)
+        case.ctx.check(self._capi.lib().tb_inject(case.ctx.handle, self._ctypes.byref(self.args), s))
+        case.n_loaded = 2 * int(self.args.n_species)
