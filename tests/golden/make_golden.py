@@ -195,6 +195,33 @@ def main(ref):
          circuit_up=circ["up"], circuit_V1=circ["V1"],
          **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
 
+    # --- vertical-ion probe (trench_charging_2d.py:1373-1439) -------------------
+    def probe_case(name, p, rho):
+        solid, mask, i0, i1 = T.build_geometry(p)
+        res = dict(params=asdict(p), solid=solid, mask=mask, i0=i0, i1=i1, rho_raw=rho, t_conv=1e-3,
+                   stopped=False, circuit=None)
+        out = T.probe_vertical_ions(res, log=lambda s: None)
+        arrays = {}
+        for label in ("charged", "uncharged"):
+            r = out[label]
+            for k in ("hits", "status", "hit_cells", "endpoints", "final_velocity", "angle_deg",
+                      "impact_energy_eV", "bottom_flux", "phi", "Ex", "Ey"):
+                arrays[f"{label}_{k}"] = np.asarray(r[k])
+            arrays[f"{label}_scalars"] = np.array([r["bottom_fraction"], r["escaped"], r["lost"]], dtype=float)
+            arrays[f"{label}_path_lengths"] = np.array([len(v) for v in r["paths"]])
+            arrays[f"{label}_paths"] = np.concatenate(r["paths"])
+        save(f"probe_{name}.npz", params=params_json(p), solid=solid, mask=mask, rho_raw=rho, **arrays)
+
+    pt = replace(taper, field_mode="floating", substrate_voltage=0, mask_voltage=0, probe_ions=224,
+                 probe_trajectories=12)
+    probe_case("taper_empty", pt, np.zeros(T.build_geometry(pt)[0].shape))
+    ps = replace(P(), nx=20, trench_w=6, trench_d=12, floor_t=4, mask_t=4, n_vac=8, bias="dc", sigma_s=0,
+                 probe_ions=120, probe_trajectories=8, max_steps=800)
+    solid, mask, i0, i1 = T.build_geometry(ps)
+    rho = np.zeros(solid.shape)
+    rho[i0 - 1, ps.floor_t:ps.floor_t + ps.trench_d] = 1e7
+    probe_case("small_charged", ps, rho)
+
     # --- field-side cases -----------------------------------------------------
     for name, p in {"floating": runs["floating_leak"], "fixed": runs["fixed_leak"],
                     "dielectric": runs["dielectric_leak"],

@@ -164,3 +164,39 @@ def test_rf_batch_loop_matches_reference_run(case_cls):
     np.testing.assert_allclose(res["mean_phi"], g["mean_phi"], rtol=1e-10, atol=1e-8)
     for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
         np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])
+
+
+@pytest.mark.parametrize("mode", ["floating", "fixed", "dielectric"])
+def test_resume_equals_continuous_run(case_cls, tmp_path, mode):
+    """Split-and-resume equals the continuous run bit for bit (tests/test_resume.py:35-49),
+    through the NPZ file."""
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc",
+                sigma_s=1e-14, n_per_batch=1500, n_batches=3, seed=4)
+    if mode == "fixed":
+        p = replace(p, field_mode="fixed", substrate_voltage=-20, mask_voltage=-10)
+    elif mode == "dielectric":
+        p = replace(p, mask_type="dielectric")
+    full = case_cls(p, max_batches=4).run()
+    a = case_cls(p, max_batches=4)
+    rng = np.random.default_rng(p.seed)
+    a.run(n_batches=1, rng=rng)
+    a.save(tmp_path / "part.npz", rng=rng)
+    b = case_cls(p, max_batches=4)
+    cont = b.run(n_batches=2, resume=case_cls.load_checkpoint(tmp_path / "part.npz"))
+    np.testing.assert_array_equal(cont["rho_raw"], full["rho_raw"])
+    np.testing.assert_array_equal(cont["mean_phi"], full["mean_phi"])
+    np.testing.assert_array_equal(cont["Ex"], full["Ex"])
+    for k in full["hist"]:
+        np.testing.assert_array_equal(cont["hist"][k], full["hist"][k])
+
+
+def test_resume_from_a_reference_result(case_cls):
+    """A reference run() result (rho_raw, history, PCG64 state) continues on the device:
+    the state after 4 reference batches, restored, gives the reference's next potentials."""
+    g = load_golden("run_floating_leak.npz")
+    p = g["p"]
+    case = case_cls(p, precision="f64", max_batches=8)
+    hist = {k[5:]: g[k] for k in g if k.startswith("hist_")}
+    case.restore(dict(rho_raw=g["rho_raw"], hist=hist))
+    np.testing.assert_allclose(case.full_potential(), g["mean_phi"], rtol=1e-10, atol=1e-8)
+    assert case.batches_done() == p.n_batches

@@ -240,3 +240,70 @@ class FieldSolver:
         x = self.solve_rows(rows)
         x = x[0] if one else x.T
         return x.cpu().numpy() if host else x
+
+
+def setup_fields(p, solid, mask, circuit=None, device=0, max_rhs=64):
+    """The reference's setup_fields (trench_charging_2d.py:340-413) on the device solver:
+    returns dict(solve, cond, eps, external, boundary_rhs, volts, floating, rf, solver),
+    with `solve` a FieldSolver.solve (b of A phi = b, flat or column-stacked)."""
+    from .tracer import Context
+    volts = field_voltages(p, mask, circuit)
+    driven = p.field_mode != "floating"
+    cond = mask if p.mask_type == "conductor" else np.zeros_like(mask)
+    from .geometry import permittivity
+    eps = permittivity(solid, mask, p)
+    ctx = Context(~solid, device, p.dx)
+    solver = FieldSolver(ctx, p, eps, cond, driven, max_rhs=max_rhs)
+    nx, ny = solid.shape
+    if driven and cond.any():
+        phi_cond = cond.astype(float) * volts["mask"]
+        mask_rhs = -apply_matrix(solver.diag, solver.ce, solver.cn, phi_cond)
+    else:
+        phi_cond = np.zeros((nx, ny))
+        mask_rhs = np.zeros((nx, ny))
+    rhs = boundary_rhs(p, eps, volts)
+    external = (solver.solve((rhs + mask_rhs).ravel()) + phi_cond.ravel()).reshape(nx, ny)
+    fields = dict(solve=solver.solve, solver=solver, ctx=ctx, cond=cond, eps=eps, external=external,
+                  boundary_rhs=rhs, volts=volts, floating=bool(cond.any() and not driven), rf=None)
+    if p.field_mode == "circuit_rf":
+        t = np.asarray(circuit["t"])
+        period = (t[1] - t[0]) * t.size
+        wave = np.column_stack((circuit["uw"] - circuit["up"], circuit["um"] - circuit["up"]))
+        mean = wave.mean(axis=0)
+        basis, rhs_basis = [], []
+        for vs, vm in ((1.0, 0.0), (0.0, 1.0)):
+            brhs = boundary_rhs(p, eps, dict(substrate=vs, mask=vm, top=0.0), fixed_sides=False)
+            bc = cond.astype(float) * vm
+            b = brhs - apply_matrix(solver.diag, solver.ce, solver.cn, bc)
+            basis.append((solver.solve(b.ravel()) + bc.ravel()).reshape(nx, ny))
+            rhs_basis.append(brhs)
+        basis = np.array(basis)
+        electric = [compute_field(v, ~solid, p, 0.0) for v in basis]
+        dt_max = period / p.rf_time_steps
+        if p.rf_wave == "pulse":
+            dt_max = min(dt_max, p.rf_rise / 8)
+        fields["rf"] = dict(period=period, wave=wave - mean, phi=basis, Ex=np.array([e[0] for e in electric]),
+                            Ey=np.array([e[1] for e in electric]), dt_max=dt_max, boundary_rhs=np.array(rhs_basis))
+    return fields
+
+
+def rf_coefficients(rf, at):
+    """Periodic linear interpolation of the voltage deltas (trench_rf.py:5-11)."""
+    wave = rf["wave"]
+    f = (np.asarray(at) % rf["period"]) / rf["period"] * len(wave)
+    i = np.floor(f).astype(np.int64) % len(wave)
+    w = (f - np.floor(f))[..., None]
+    return wave[i] * (1 - w) + wave[(i + 1) % len(wave)] * w
+
+
+def field_snapshot(fields, mean_phi, p):
+    """Display-phase potential of circuit_rf (trench_charging_2d.py:416-426)."""
+    if fields["rf"] is None:
+        return mean_phi, fields["external"], fields["boundary_rhs"], fields["volts"]
+    rf = fields["rf"]
+    delta = rf_coefficients(rf, (p.rf_phase % 360) / 360 * rf["period"])
+    shift = np.einsum("i,ijk->jk", delta, rf["phi"])
+    rhs = fields["boundary_rhs"] + np.einsum("i,ijk->jk", delta, rf["boundary_rhs"])
+    volts = {**fields["volts"], "substrate": fields["volts"]["substrate"] + float(delta[0]),
+             "mask": fields["volts"]["mask"] + float(delta[1])}
+    return mean_phi + shift, fields["external"] + shift, rhs, volts

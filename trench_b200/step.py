@@ -14,6 +14,8 @@ the implicit leakage operator M = inv(I - dt G_leak P) (trench_charging_2d.py:76
 from multigrid solves on the GPU.
 """
 import ctypes
+import json
+from dataclasses import asdict, is_dataclass
 
 import numpy as np
 import torch
@@ -25,6 +27,7 @@ from .params import E_CHARGE, EPS0, WALL_MODELS, is_tapered
 from .tracer import DEFAULT_VSCALE, Context, _ptr
 
 HIST_SCALARS = ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost", "leak", "particle_steps")
+CHECKPOINT_VERSION = 1
 
 
 class ChargingCase:
@@ -366,16 +369,93 @@ class ChargingCase:
     def fields(self):
         return (self.ex.cpu().numpy().reshape(self.nx, self.ny), self.ey.cpu().numpy().reshape(self.nx, self.ny))
 
-    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None):
-        """The reference batch loop (trench_charging_2d.py:1225-1285) with host injection."""
+    # ---- checkpoint / resume ---------------------------------------------------------
+    def checkpoint(self, rng=None, phase_rng=None):
+        """State to continue from: the surface charge (as the reference's full-grid rho_raw),
+        the history and the generator states (trench_charging_2d.py:1361-1364).  Everything
+        else on the device is recomputed from the charge."""
+        self.check()
+        params = asdict(self.p) if is_dataclass(self.p) else dict(vars(self.p))
+        return dict(rho_raw=self.rho(), hist=self.history(), params=params,
+                    checkpoint=dict(version=CHECKPOINT_VERSION, batches_completed=self.batches_done(),
+                                    rng_state=rng.bit_generator.state if rng is not None else None,
+                                    phase_rng_state=phase_rng.bit_generator.state if phase_rng is not None
+                                    else None))
+
+    def restore(self, res):
+        """Continue from a checkpoint of this backend or a reference result of the same case
+        (keys rho_raw, hist): charge, history rows and batch counter."""
+        rho = np.asarray(res["rho_raw"], dtype=np.float64)
+        if rho.shape != (self.nx, self.ny) or not np.isfinite(rho).all():
+            raise ValueError("the checkpoint's charge does not match this geometry")
+        off = np.ones(self.n, bool)
+        off[self.S] = False
+        if np.any(rho.ravel()[off] != 0):
+            raise ValueError("the checkpoint holds charge outside the surface cells")
+        hist = res.get("hist", {})
+        t = np.asarray(hist.get("t", []))
+        done = len(t)
+        if done > self.max_batches:
+            raise ValueError("the checkpoint has more batches than this case's history holds")
+        rows = np.zeros((done, self.hist_cols))
+        for i, k in enumerate(HIST_SCALARS):
+            if k in hist:
+                rows[:, i] = np.asarray(hist[k], dtype=np.float64)[:done]
+        for j, k in enumerate(self.probes):
+            if k in hist:
+                rows[:, len(HIST_SCALARS) + j] = np.asarray(hist[k], dtype=np.float64)[:done]
+        with torch.cuda.device(self.dev):
+            self.rho_s.copy_(torch.from_numpy(rho.ravel()[self.S].copy()))
+            self.hist.zero_()
+            if done:
+                self.hist[:done].copy_(torch.from_numpy(rows))
+            self.batch.fill_(done - 1)
+            self._potential()
+            torch.cuda.current_stream(self.dev).synchronize()
+
+    def save(self, path, rng=None, phase_rng=None):
+        """NPZ without pickled objects: arrays plus JSON text (like trench_charging_2d.py:1720-1733)."""
+        ck = self.checkpoint(rng, phase_rng)
+        np.savez(path, rho_raw=ck["rho_raw"], params_json=json.dumps(ck["params"]),
+                 checkpoint_json=json.dumps(ck["checkpoint"]),
+                 **{f"hist_{k}": v for k, v in ck["hist"].items()})
+
+    @staticmethod
+    def load_checkpoint(path):
+        """Read a file written by save()."""
+        with np.load(path, allow_pickle=False) as d:
+            res = dict(rho_raw=d["rho_raw"], params=json.loads(str(d["params_json"])),
+                       checkpoint=json.loads(str(d["checkpoint_json"])),
+                       hist={k[5:]: d[k] for k in d.files if k.startswith("hist_")})
+        return res
+
+    @staticmethod
+    def restore_rng(state):
+        """A numpy Generator positioned at a saved PCG64 state (trench_charging_2d.py:1012-1031)."""
+        rng = np.random.default_rng()
+        rng.bit_generator.state = state
+        return rng
+
+    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None, resume=None):
+        """The reference batch loop (trench_charging_2d.py:1225-1285) with host injection;
+        `resume` (a checkpoint or loaded file) continues a saved run for n_batches more."""
         p = self.p
         n_batches = p.n_batches if n_batches is None else n_batches
+        phase_rng = None
+        if resume is not None:
+            self.restore(resume)
+            ck = resume.get("checkpoint") or {}
+            if rng is None and ck.get("rng_state"):
+                rng = self.restore_rng(ck["rng_state"])
+            if self.rf is not None and ck.get("phase_rng_state"):
+                phase_rng = self.restore_rng(ck["phase_rng_state"])
         rng = np.random.default_rng(p.seed) if rng is None else rng
         if p.field_mode in ("circuit", "circuit_rf") and ion_energy is None and ion_velocity is None:
             # ions start at the plasma potential with the Bohm energy (trench_charging_2d.py:1135-1139)
             ion_energy = lambda r, k: np.full(k, p.electron_temp_eV / 2)
-        phase_rng = (np.random.default_rng(np.random.SeedSequence([p.seed, 0x5246]))
-                     if self.rf is not None else None)
+        if phase_rng is None and self.rf is not None:
+            phase_rng = np.random.default_rng(np.random.SeedSequence([p.seed, 0x5246]))
+        self._rngs = (rng, phase_rng)
         with torch.cuda.device(self.dev):
             for b in range(n_batches):
                 parts = inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity)
@@ -389,5 +469,6 @@ class ChargingCase:
                     log(f"[{b + 1}/{n_batches}]")
             self.check()
         ex, ey = self.fields()
+        ck = self.checkpoint(rng, phase_rng)["checkpoint"]
         return dict(rho_raw=self.rho(), mean_phi=self.full_potential(), Ex=ex, Ey=ey, hist=self.history(),
-                    solid=self.solid, mask=self.mask, probes=self.probes, backend_used="b200")
+                    solid=self.solid, mask=self.mask, probes=self.probes, backend_used="b200", checkpoint=ck)
