@@ -11,9 +11,9 @@ seeded inputs.  A step is one charging batch: trace -> deposit -> leakage ->
 potential -> field, on the device, replayed from a CUDA graph.
 
 value: traced particles per second over the timed steps (device-resident inputs,
-L2 flushed between steps, CUDA events).  e2e: the same through ChargingCase.load
-+ step with the batch copied from pinned host memory every step and the history
-row read back.  Under torchrun every rank runs its own case (weak scaling, no
+L2 flushed between steps, CUDA events).  e2e: the same through the public API
+with every step's batch copied from pinned host memory (HostPipeline: the copy of
+batch k+1 overlaps batch k) and its history row read back, timed over all steps.  Under torchrun every rank runs its own case (weak scaling, no
 collective on the data path); rank 0 prints the line.
 
 --impl reference times the reference algorithm on the host cores (the FP64 C
@@ -109,6 +109,24 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def reduce_max(value, device=None):
+    """Max of a per-rank number over all ranks (the timing rule: the slowest rank sets the
+    time); identity without a process group.  Works on NCCL (device tensor) and gloo."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64,
+                     device=device if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_workload(p, rank):
+    """Weak scaling: every rank runs its own case of the same workload (own seed)."""
+    return replace(p, seed=p.seed + rank)
+
+
 def measured_peaks():
     try:
         return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
@@ -192,7 +210,7 @@ def run_b200(args, p):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
 
     n_steps = args.warmup + args.steps
-    case = ChargingCase(replace(p, seed=p.seed + rank), device=local, precision="f32", green="f64",
+    case = ChargingCase(rank_workload(p, rank), device=local, precision="f32", green="f64",
                         max_batches=2 * n_steps + 8)
     ny = case.ny
     sampler = ion_sampler(p)
@@ -262,43 +280,33 @@ def run_b200(args, p):
     torch.cuda.nvtx.range_pop()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = reduce_max(total_ms, dev)
     hist = case.history()
     steps_per_batch = hist["particle_steps"][steps_before:steps_before + args.steps]
 
-    # e2e: host buffers through the public API (H2D each step, history row D2H)
-    e2e_ms = []
-    row = torch.empty(case.hist_cols, dtype=torch.float64).pin_memory()
-    for k in range(args.steps):
-        h = host[k % pool_n]
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record()
-        case.load(*h, non_blocking=True)
-        if graph_ok:
-            case.replay()
-        else:
-            case.step(n)
-        b = case.batches_done() - 1 if False else None  # noqa: F841
-        row.copy_(case.hist[min(steps_before + args.steps + k, case.max_batches - 1)], non_blocking=True)
-        s1.record()
-        flush.zero_()
-        s1.synchronize()
-        e2e_ms.append(s0.elapsed_time(s1))
+    # e2e: host buffers through the public API: every step's batch is copied from pinned
+    # host memory (overlapping the previous step's compute) and its history row read back
+    from trench_b200.step import HostPipeline
+    pipe = HostPipeline(case, n)
+    batches = [host[k % pool_n] for k in range(args.steps)]
+    rows = torch.empty((args.steps, case.hist_cols), dtype=torch.float64).pin_memory()
+    pipe.run(batches[:2], rows[:2])                      # warm the second graph
+    torch.cuda.synchronize()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record()
+    pipe.run(batches, rows, between=flush.zero_)
+    s1.record()
+    s1.synchronize()
+    e2e_total = s0.elapsed_time(s1)
+    row = rows[0]
     # device injection: the batch is drawn on the GPU (Philox) inside the captured graph
     dinj = device_injection(case, p, args.steps)
     clk = clocks.stop()
     case.check()
     h2d = sum(t.numel() * t.element_size() for t in host[0])
     d2h = row.numel() * row.element_size()
-    e2e_total = float(sum(e2e_ms))
-    if world > 1:
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+    e2e_total = reduce_max(e2e_total, dev)
 
     if rank != 0:
         if world > 1:

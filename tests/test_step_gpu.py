@@ -200,3 +200,26 @@ def test_resume_from_a_reference_result(case_cls):
     case.restore(dict(rho_raw=g["rho_raw"], hist=hist))
     np.testing.assert_allclose(case.full_potential(), g["mean_phi"], rtol=1e-10, atol=1e-8)
     assert case.batches_done() == p.n_batches
+
+
+def test_host_pipeline_equals_sequential_batches(case_cls):
+    """Copies overlapped with compute (two buffer sets, one graph each) give the same
+    results as loading and stepping one batch after the other."""
+    import torch
+    from trench_b200.step import HostPipeline
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc",
+                sigma_s=1e-14, n_per_batch=3000, n_batches=4)
+    rng = np.random.default_rng(8)
+    a, b = case_cls(p, max_batches=6), case_cls(p, max_batches=6)
+    host = [[torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+             for v in inject.inject(p, p.n_per_batch, a.ny, rng)] for _ in range(4)]
+    for h in host:
+        a.load(*h)
+        a.step()
+    b.load(*host[0])
+    rows = torch.empty((4, b.hist_cols), dtype=torch.float64).pin_memory()
+    HostPipeline(b, 2 * p.n_per_batch).run(host, rows)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(a.rho(), b.rho())
+    np.testing.assert_array_equal(rows.numpy(), b.hist[:4].cpu().numpy())
+    np.testing.assert_array_equal(a.history()["ratio_e_bottom"], b.history()["ratio_e_bottom"])

@@ -143,6 +143,7 @@ class ChargingCase:
             self.totals = torch.zeros(8, dtype=torch.int64, device=dev)
             self.X = [torch.zeros(cap, dtype=f64, device=dev) for _ in range(5)]  # x, y, vx, vy, qm
             self.SPC = torch.zeros(cap, dtype=torch.int8, device=dev)
+            self._inputs = [(self.X, self.SPC)]   # input buffer sets (a second one for pipelining)
             self.status = torch.full((cap,), 3, dtype=torch.int8, device=dev)
             self.steps = torch.zeros(cap, dtype=torch.int32, device=dev)
             self.n_loaded = 0
@@ -279,10 +280,20 @@ class ChargingCase:
         self.SPC[:n].copy_(t, non_blocking=non_blocking)
         self.n_loaded = n
 
-    def step(self, n=None):
-        """One charging batch on the current stream (trace, deposit, leakage, conductor, potential, field)."""
+    def add_input_buffer(self):
+        """A second set of particle input buffers, so the next batch can be copied in while
+        the current one runs (see HostPipeline)."""
+        if len(self._inputs) < 2:
+            X = [torch.zeros(self.capacity, dtype=torch.float64, device=self.dev) for _ in range(5)]
+            self._inputs.append((X, torch.zeros(self.capacity, dtype=torch.int8, device=self.dev)))
+        return self._inputs[1]
+
+    def step(self, n=None, buffer=0):
+        """One charging batch on the current stream (trace, deposit, leakage, conductor, potential, field),
+        reading the particles from input buffer set `buffer`."""
         L = _capi.lib()
         n = self.n_loaded if n is None else n
+        X, SPC = self._inputs[buffer]
         p = self.p
         s = self._stream()
         self.status[:n].fill_(3)
@@ -291,8 +302,8 @@ class ChargingCase:
         self.totals.zero_()
         a = self._args
         a.n = n
-        a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in self.X)
-        a.d_spc = _ptr(self.SPC)
+        a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in X)
+        a.d_spc = _ptr(SPC)
         a.d_ex, a.d_ey = _ptr(self.ex), _ptr(self.ey)
         bar = p.wall_model == "barrier"
         a.d_phi, a.d_wface = (_ptr(self.phi), _ptr(self.t_wface)) if bar else (None, None)
@@ -323,17 +334,18 @@ class ChargingCase:
         self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
         self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
 
-    def capture(self, n=None):
-        """Capture one batch (for n particles already in the buffers) as a CUDA graph."""
+    def capture(self, n=None, buffer=0):
+        """Capture one batch (for n particles in input buffer set `buffer`) as a CUDA graph."""
         n = self.n_loaded if n is None else n
         side = torch.cuda.Stream(self.dev)
         side.wait_stream(torch.cuda.current_stream(self.dev))
         g = torch.cuda.CUDAGraph()
         with torch.cuda.stream(side):
             with torch.cuda.graph(g, stream=side):
-                self.step(n)
+                self.step(n, buffer)
         torch.cuda.current_stream(self.dev).wait_stream(side)
-        self._graph = g
+        if buffer == 0:
+            self._graph = g
         return g
 
     def replay(self):
@@ -472,3 +484,48 @@ class ChargingCase:
         ck = self.checkpoint(rng, phase_rng)["checkpoint"]
         return dict(rho_raw=self.rho(), mean_phi=self.full_potential(), Ex=ex, Ey=ey, hist=self.history(),
                     solid=self.solid, mask=self.mask, probes=self.probes, backend_used="b200", checkpoint=ck)
+
+
+class HostPipeline:
+    """Batches from pinned host memory with the copy of batch k+1 overlapping the
+    compute of batch k: two input buffer sets, one CUDA graph per set, a copy stream.
+    The reference's loop (trench_charging_2d.py:1225-1285) copies and computes one
+    batch after the other."""
+
+    def __init__(self, case, n):
+        self.case = case
+        self.n = int(n)
+        case.add_input_buffer()
+        self.graphs = [case.capture(self.n, 0), case.capture(self.n, 1)]
+        self.copy = torch.cuda.Stream(case.dev)
+        self.copied = [torch.cuda.Event(), torch.cuda.Event()]
+        self.done = [torch.cuda.Event(), torch.cuda.Event()]
+
+    def _stage(self, k, batch, after):
+        X, SPC = self.case._inputs[k % 2]
+        self.copy.wait_event(after)
+        with torch.cuda.stream(self.copy):
+            for dst, src in zip(X + [SPC], batch):
+                dst[:self.n].copy_(src, non_blocking=True)
+            self.copied[k % 2].record(self.copy)
+
+    def run(self, batches, rows=None, between=None):
+        """batches: list of (x, y, vx, vy, qm, spc) pinned host tensors of n particles each.
+        rows: optional pinned (len(batches), hist_cols) tensor receiving each batch's
+        history row.  between: optional callable run on the compute stream between batches."""
+        comp = torch.cuda.current_stream(self.case.dev)
+        start = torch.cuda.Event()
+        start.record(comp)
+        self._stage(0, batches[0], start)
+        for k in range(len(batches)):
+            comp.wait_event(self.copied[k % 2])
+            if k + 1 < len(batches):
+                # buffer (k+1)%2 is free once batch k-1 has finished with it
+                self._stage(k + 1, batches[k + 1], self.done[(k + 1) % 2] if k >= 1 else start)
+            self.graphs[k % 2].replay()
+            self.done[k % 2].record(comp)
+            if rows is not None:
+                last = self.case.batch.clamp(0, self.case.max_batches - 1).long()
+                rows[k].copy_(self.case.hist.index_select(0, last).squeeze(0), non_blocking=True)
+            if between is not None:
+                between()
