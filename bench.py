@@ -211,7 +211,7 @@ def run_b200(args, p):
 
     n_steps = args.warmup + args.steps
     case = ChargingCase(rank_workload(p, rank), device=local, precision="f32", green="f64",
-                        max_batches=2 * n_steps + 8)
+                        max_batches=2 * n_steps + 8, autotune=True)
     ny = case.ny
     sampler = ion_sampler(p)
     rng = np.random.default_rng(100 + rank)
@@ -228,6 +228,7 @@ def run_b200(args, p):
     t0e = torch.cuda.Event(enable_timing=True, external=True)
     t1e = torch.cuda.Event(enable_timing=True, external=True)
     case.load(*dev_pool[0])
+    case.autotune_tracer(n)                   # launch shape of the tracer (untimed)
     case.step()                               # eager first batch (warm-up 1)
     torch.cuda.synchronize()
     case.trace_events = (t0e, t1e)
@@ -339,7 +340,9 @@ def run_b200(args, p):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config(p, {"l2": "flushed between timed steps (256 MiB write)",
                                  "graph": graph_ok, "precision": "f32 tracer, f64 Green's operator, "
-                                 "f64 charge/leakage/conductor", "parallelism": f"{world} independent cases"}),
+                                 "f64 charge/leakage/conductor", "parallelism": f"{world} independent cases",
+                                 "tracer_shape": list(case.tuning.get("tracer_shape", ())),
+                                 "poisson_schedule": list(case.tuning.get("poisson_schedule", ()))}),
             "batches_per_s": 1000.0 * args.steps * world / total_ms,
             "e2e": {"value": particles / (e2e_total / 1000.0), "unit": "particles/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

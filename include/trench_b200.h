@@ -97,6 +97,11 @@ int tb_set_fields(tb_ctx *ctx, const double *d_ex, const double *d_ey, const dou
  * trace_particles (trench_trace.cu:70-193). */
 int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream);
 
+/* Launch shape of the FP32 tracer on this context: CTA size 512, 768 or 1024 threads
+ * and 1 or 2 CTAs per SM (2 only where two shared-memory fields fit on an SM).
+ * Chosen by the autotuner (ChargingCase.autotune); default 1024 x 1. */
+int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
+
 /* Synchronise `stream`, then read and clear the context's device-side check flag:
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the
  * grid, a bulk copy that did not complete in its bounded wait). */
@@ -110,6 +115,9 @@ int tb_check(tb_ctx *ctx, void *stream);
  * and solve of make_solver / setup_fields (trench_charging_2d.py:297-309, 378-392). */
 int tb_poisson_setup(tb_ctx *ctx, const double *h_diag, const double *h_ke, const double *h_kn,
                      const uint8_t *h_fixed, int max_rhs);
+/* V-cycle schedule: smoothing sweeps before/after the coarse correction and on the
+ * coarsest level (defaults 1, 1, 16).  Chosen by the autotuner (FieldSolver.autotune). */
+int tb_poisson_schedule(tb_ctx *ctx, int pre, int post, int coarse_sweeps);
 /* Number of multigrid levels built by tb_poisson_setup (0 before setup). */
 int tb_poisson_levels(const tb_ctx *ctx);
 /* Solve L x = b for nrhs right-hand sides, d_b and d_x (nrhs, nx*ny) FP64; d_x is

@@ -223,3 +223,28 @@ def test_host_pipeline_equals_sequential_batches(case_cls):
     np.testing.assert_array_equal(a.rho(), b.rho())
     np.testing.assert_array_equal(rows.numpy(), b.hist[:4].cpu().numpy())
     np.testing.assert_array_equal(a.history()["ratio_e_bottom"], b.history()["ratio_e_bottom"])
+
+
+def test_autotuners_pick_a_shape_and_keep_results(case_cls):
+    """Every tracer launch shape gives the same counts (deterministic tracing); the
+    multigrid schedule autotuner keeps the solution."""
+    import torch
+    p = replace(Params(), nx=60, trench_w=20, trench_d=80, floor_t=10, mask_t=20, n_vac=40, bias="dc",
+                mask_type="dielectric", n_per_batch=20000, n_batches=2)
+    tuned = case_cls(p, autotune=True)
+    plain = case_cls(p)
+    np.testing.assert_allclose(tuned.external, plain.external, rtol=0, atol=1e-9)
+    parts = inject.inject(p, p.n_per_batch, tuned.ny, np.random.default_rng(3))
+    tuned.load(*parts)
+    timings = tuned.autotune_tracer()
+    assert set(timings) == set(tuned.TRACER_SHAPES)
+    counts = []
+    from trench_b200 import _capi
+    for shape in tuned.TRACER_SHAPES:
+        assert _capi.lib().tb_set_tuning(tuned.ctx.handle, *shape) == 0
+        tuned._trace_only(2 * p.n_per_batch)
+        torch.cuda.synchronize()
+        counts.append(tuned.counts.cpu().numpy().copy())
+    for c in counts[1:]:
+        np.testing.assert_array_equal(c, counts[0])
+    assert "poisson_schedule" in tuned.tuning and "tracer_shape" in tuned.tuning

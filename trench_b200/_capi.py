@@ -107,8 +107,10 @@ SIGNATURES = {
     "tb_set_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _vp]),
     "tb_trace": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs), ctypes.c_int, _vp]),
     "tb_check": (ctypes.c_int, [_vp, _vp]),
+    "tb_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "tb_poisson_setup": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int]),
     "tb_poisson_levels": (ctypes.c_int, [_vp]),
+    "tb_poisson_schedule": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "tb_poisson_solve": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _dbl, ctypes.c_int, ctypes.c_int,
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_dbl), _vp]),
     "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),

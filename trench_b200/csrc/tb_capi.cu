@@ -65,6 +65,7 @@ extern "C" int tb_create(tb_ctx **out, int device, int nx, int ny, double dx, co
     snprintf(c->name, sizeof(c->name), "%.120s", prop.name);
     c->num_sms = prop.multiProcessorCount;
     c->max_smem = (int)prop.sharedMemPerBlockOptin;
+    c->smem_per_sm = (int)prop.sharedMemPerMultiprocessor;
     const size_t cells = (size_t)nx * ny;
     const size_t padded = (cells + 1) & ~(size_t)1;
     e = cudaMalloc(&c->d_vac, cells);

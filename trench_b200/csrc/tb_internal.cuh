@@ -87,6 +87,9 @@ struct tb_ctx {
     int fields_ready = 0;
     int max_smem = 0;                    // opt-in shared memory per block (bytes)
     int smem_attr_bytes = 0;             // dynamic shared memory set on the FP32 tracer
+    int smem_per_sm = 0;                 // shared memory of one SM (bytes)
+    int tune_threads = 1024;             // FP32 tracer CTA size (tb_set_tuning)
+    int tune_ctas_per_sm = 1;            // FP32 tracer CTAs per SM
     tb_poisson *poisson = nullptr;        // multigrid hierarchy (tb_poisson_setup)
     char err[512] = {0};
 };

@@ -447,6 +447,17 @@ extern "C" int tb_poisson_setup(tb_ctx *ctx, const double *h_diag, const double 
     return TB_OK;
 }
 
+extern "C" int tb_poisson_schedule(tb_ctx *ctx, int pre, int post, int coarse_sweeps) {
+    if (!ctx) return TB_ERR_ARG;
+    if (!ctx->poisson) return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_schedule: call tb_poisson_setup first");
+    if (pre < 1 || pre > 8 || post < 1 || post > 8 || coarse_sweeps < 1 || coarse_sweeps > 256)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_poisson_schedule: sweeps out of range");
+    ctx->poisson->pre = pre;
+    ctx->poisson->post = post;
+    ctx->poisson->coarse_sweeps = coarse_sweeps;
+    return TB_OK;
+}
+
 extern "C" int tb_poisson_levels(const tb_ctx *ctx) {
     return (ctx && ctx->poisson) ? (int)ctx->poisson->lev.size() : 0;
 }

@@ -308,8 +308,8 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp) {
     }
 }
 
-template <bool SMEM>
-__global__ void __launch_bounds__(F32_THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
+template <bool SMEM, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
     const tb_fcell *fieldp = k.field;
@@ -415,7 +415,12 @@ int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const
 // attribute calls; the attribute is per function and device, always this value.
 int tb_configure_trace_f32(tb_ctx *ctx) {
     const int limit = ctx->max_smem - 1024;
-    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      limit));
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, 768>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      limit));
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      limit));
     TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       limit));
     ctx->smem_attr_bytes = limit;
@@ -461,14 +466,25 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
-    long long want = (a->n + F32_THREADS - 1) / F32_THREADS;
-    int blocks = (int)(want < ctx->num_sms ? want : ctx->num_sms);
+    // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning); several
+    // CTAs per SM only when their shared-memory fields fit side by side
+    const int threads = ctx->tune_threads;
+    int per_sm = ctx->tune_ctas_per_sm;
+    if (smem && (long long)per_sm * (k.bytes + 1024) > ctx->smem_per_sm) per_sm = 1;
+    long long want = (a->n + threads - 1) / threads;
+    long long cap = (long long)ctx->num_sms * per_sm;
+    int blocks = (int)(want < cap ? want : cap);
     if (blocks < 1) blocks = 1;
-    if (smem) {
-        trace_f32_kernel<true><<<blocks, F32_THREADS, k.bytes, s>>>(k);
-    } else {
-        trace_f32_kernel<false><<<blocks, F32_THREADS, 0, s>>>(k);
-    }
+    const size_t shm = smem ? (size_t)k.bytes : 0;
+#define TB_LAUNCH_F32(T)                                                                        \
+    do {                                                                                        \
+        if (smem) trace_f32_kernel<true, T><<<blocks, T, shm, s>>>(k);                         \
+        else trace_f32_kernel<false, T><<<blocks, T, 0, s>>>(k);                               \
+    } while (0)
+    if (threads == 512) TB_LAUNCH_F32(512);
+    else if (threads == 768) TB_LAUNCH_F32(768);
+    else TB_LAUNCH_F32(1024);
+#undef TB_LAUNCH_F32
     TB_CUDA(ctx, cudaGetLastError());
     return TB_OK;
 }
@@ -715,5 +731,15 @@ extern "C" int tb_pack_check(tb_pack *p, void *stream) {
         cudaMemsetAsync(p->d_err, 0, sizeof(int), s);
         return pack_fail(p, TB_ERR_KERNEL, "a kernel check failed in the case pack");
     }
+    return TB_OK;
+}
+
+
+extern "C" int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm) {
+    if (!ctx) return TB_ERR_ARG;
+    if ((threads != 512 && threads != 768 && threads != 1024) || ctas_per_sm < 1 || ctas_per_sm > 2)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_set_tuning: threads must be 512, 768 or 1024 and CTAs per SM 1 or 2");
+    ctx->tune_threads = threads;
+    ctx->tune_ctas_per_sm = ctas_per_sm;
     return TB_OK;
 }

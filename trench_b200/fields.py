@@ -174,6 +174,8 @@ class FieldSolver:
         kn = self.cn * self.dx2
         fixed = self.cond.astype(np.uint8) if self.mode != "none" else np.zeros((self.nx, self.ny), np.uint8)
         self.max_rhs = int(max_rhs)
+        self.inner = 12             # FP32 PCG iterations per FP64 refinement step
+        self.schedule_used = (1, 1, 16, 12)
         L = _capi.lib()
         f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
         ctx.check(L.tb_poisson_setup(ctx.handle, f(d).ctypes.data_as(ctypes.c_void_p),
@@ -209,13 +211,39 @@ class FieldSolver:
             b = bp[s:e].contiguous()
             x = out[s:e].contiguous()
             self.ctx.check(L.tb_poisson_solve(self.ctx.handle, e - s, ctypes.c_void_p(b.data_ptr()),
-                                              ctypes.c_void_p(x.data_ptr()), self.RTOL, 40, 12,
+                                              ctypes.c_void_p(x.data_ptr()), self.RTOL, 40, self.inner,
                                               ctypes.byref(iters), ctypes.byref(resid),
                                               ctypes.c_void_p(stream.cuda_stream)))
             out[s:e] = x
             self.last_iters = max(self.last_iters, iters.value)
             self.last_resid = max(self.last_resid, resid.value)
         return out
+
+    # candidate V-cycle schedules: (pre, post, coarsest sweeps, PCG iterations per refinement)
+    SCHEDULES = ((1, 1, 16, 12), (2, 2, 16, 8), (1, 1, 8, 16), (2, 2, 32, 6), (3, 3, 16, 6))
+
+    def set_schedule(self, pre, post, coarse, inner):
+        self.ctx.check(_capi.lib().tb_poisson_schedule(self.ctx.handle, int(pre), int(post), int(coarse)))
+        self.inner = int(inner)
+        self.schedule_used = (int(pre), int(post), int(coarse), int(inner))
+
+    def autotune(self, b_rows, reps=2):
+        """Times the candidate schedules on the right-hand sides b_rows (k, n) (SPD form,
+        zero on fixed cells), keeps the fastest and returns {schedule: seconds}."""
+        import time
+        timings = {}
+        for sch in self.SCHEDULES:
+            self.set_schedule(*sch)
+            best = float("inf")
+            for _ in range(reps):
+                torch.cuda.synchronize(self.dev)
+                t0 = time.perf_counter()
+                self._solve_spd(b_rows)
+                torch.cuda.synchronize(self.dev)
+                best = min(best, time.perf_counter() - t0)
+            timings[sch] = best
+        self.set_schedule(*min(timings, key=timings.get))
+        return timings
 
     def solve_rows(self, b):
         """A phi = b for the rows of b (k, n) given as a device tensor; returns (k, n)."""

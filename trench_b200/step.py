@@ -32,7 +32,7 @@ CHECKPOINT_VERSION = 1
 
 class ChargingCase:
     def __init__(self, p, device=0, precision="f32", green="f64", circuit=None, max_batches=None,
-                 capacity=None, vscale=DEFAULT_VSCALE, max_rhs=64):
+                 capacity=None, vscale=DEFAULT_VSCALE, max_rhs=64, autotune=False):
         if precision not in _capi.PRECISION:
             raise ValueError(f"precision must be one of {tuple(_capi.PRECISION)}")
         if green not in ("f32", "f64"):
@@ -83,6 +83,15 @@ class ChargingCase:
             probe_flat = np.array([ix * ny + iy for ix, iy in self.probes.values()], dtype=np.int64)
             rows = np.union1d(np.union1d(np.flatnonzero(vac.ravel()), S), probe_flat)
             self.rows = rows
+            self.tuning = {}
+            if autotune:
+                # the multigrid schedule for the surface Green's solves: timed on a block of them
+                k = min(self.solver.max_rhs, m)
+                b = torch.zeros((k, self.n), dtype=torch.float64, device=dev)
+                b[torch.arange(k, device=dev), torch.from_numpy(S[:k]).to(dev)] = p.dx ** 2 / EPS0
+                b = torch.where(self.solver.cond_t[None, :], torch.zeros_like(b), b)
+                self.tuning["poisson"] = {str(k_): v for k_, v in self.solver.autotune(b).items()}
+            self.tuning["poisson_schedule"] = self.solver.schedule_used
             self._build_green(rows, green)
             # leakage (trench_charging_2d.py:768-803)
             self.leak_M = self.leak_h = None
@@ -288,18 +297,11 @@ class ChargingCase:
             self._inputs.append((X, torch.zeros(self.capacity, dtype=torch.int8, device=self.dev)))
         return self._inputs[1]
 
-    def step(self, n=None, buffer=0):
-        """One charging batch on the current stream (trace, deposit, leakage, conductor, potential, field),
-        reading the particles from input buffer set `buffer`."""
-        L = _capi.lib()
-        n = self.n_loaded if n is None else n
-        X, SPC = self._inputs[buffer]
+    def _fill_args(self, n, buffer=0):
+        """Tracer arguments of one batch of n particles in input buffer set `buffer`;
+        returns the precision of the kernel that traces it."""
         p = self.p
-        s = self._stream()
-        self.status[:n].fill_(3)
-        self.steps[:n].zero_()
-        self.counts.zero_()
-        self.totals.zero_()
+        X, SPC = self._inputs[buffer]
         a = self._args
         a.n = n
         a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in X)
@@ -324,6 +326,20 @@ class ChargingCase:
             a.period, a.dt_max = self.rf["period"], self.rf["dt_max"]
             a.bound_vs, a.bound_vm = self.rf_bound
             a.d_clock = _ptr(self.clock)
+        return precision
+
+    def step(self, n=None, buffer=0):
+        """One charging batch on the current stream (trace, deposit, leakage, conductor, potential, field),
+        reading the particles from input buffer set `buffer`."""
+        L = _capi.lib()
+        n = self.n_loaded if n is None else n
+        s = self._stream()
+        self.status[:n].fill_(3)
+        self.steps[:n].zero_()
+        self.counts.zero_()
+        self.totals.zero_()
+        a = self._args
+        precision = self._fill_args(n, buffer)
         ev = getattr(self, "trace_events", None)
         if ev is not None:
             ev[0].record()
@@ -333,6 +349,52 @@ class ChargingCase:
             ev[1].record()
         self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
         self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
+
+    TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2))
+
+    def autotune_tracer(self, n=None, reps=2):
+        """Times the tracer's launch shapes (CTA size, CTAs per SM) on the loaded batch and
+        keeps the fastest.  Traces only: the charge state is not changed (the trace is
+        deterministic, so every shape gives the same counts)."""
+        L = _capi.lib()
+        n = self.n_loaded if n is None else n
+        p = self.p
+        timings = {}
+        saved = self.trace_events
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        self.trace_events = (e0, e1)
+        try:
+            for threads, per_sm in self.TRACER_SHAPES:
+                self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
+                best = float("inf")
+                for _ in range(reps):
+                    self._trace_only(n)
+                    e1.synchronize()
+                    best = min(best, e0.elapsed_time(e1))
+                timings[(threads, per_sm)] = best
+        finally:
+            self.trace_events = saved
+        shape = min(timings, key=timings.get)
+        self.ctx.check(L.tb_set_tuning(self.ctx.handle, *shape))
+        self.tuning["tracer"] = {f"{t}x{c}": v for (t, c), v in timings.items()}
+        self.tuning["tracer_shape"] = shape
+        return timings
+
+    def _trace_only(self, n):
+        """The tracer launch of step() alone (counts and status are overwritten by the next step)."""
+        L = _capi.lib()
+        s = self._stream()
+        self.status[:n].fill_(3)
+        self.steps[:n].zero_()
+        self.counts.zero_()
+        self.totals.zero_()
+        precision = self._fill_args(n)
+        ev = self.trace_events
+        if ev is not None:
+            ev[0].record()
+        self.ctx.check(L.tb_trace(self.ctx.handle, ctypes.byref(self._args), _capi.PRECISION[precision], s))
+        if ev is not None:
+            ev[1].record()
 
     def capture(self, n=None, buffer=0):
         """Capture one batch (for n particles in input buffer set `buffer`) as a CUDA graph."""
