@@ -258,6 +258,21 @@ def main(ref):
     vals = [T.conductor_step(*c) for c in cases]
     save("conductor_step.npz", args=np.array(cases, dtype=float), values=np.array(vals))
 
+    # --- configuration 1, full run (30 batches, 10k ions + 10k electrons, DC 100 eV, angles N(0, 2 deg)) ----
+    sys.path.insert(0, str(OUT.parents[1]))
+    from trench_b200 import inject as b200_inject
+    cfg1_run = replace(cfg1, n_per_batch=10000, n_batches=30, probe_trajectories=40)
+    sampler = b200_inject.energy_angle_sampler(cfg1_run, lambda r, k: np.full(k, 100.0),
+                                               b200_inject.gaussian_angle(2.0))
+    orig_inject = T.inject
+    T.inject = lambda p_, n_, ny_, rng_, ie=None, iv=None: orig_inject(p_, n_, ny_, rng_, None, sampler)
+    try:
+        res = T.run(cfg1_run, log=lambda s: None)
+    finally:
+        T.inject = orig_inject
+    save("run_cfg1_30.npz", params=params_json(cfg1_run), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
+         solid=res["solid"], mask=res["mask"], **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
+
     # --- agreement with the reference's own regression data -------------------
     pin = {}
     data = Path(ref) / "tests" / "data"

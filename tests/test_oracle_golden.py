@@ -92,6 +92,31 @@ def test_oracle_batch_loop_matches_reference_run(name):
         np.testing.assert_array_equal(np.array(st.hist["ratio_e_bottom"]), g["ref_data_hist_ratio_e_bottom"])
 
 
+def cfg1_ion_sampler(p):
+    """DC 100 eV ions with polar angles N(0, 2 deg): the ion source of the 30-batch
+    80x200 floating-mask fixture."""
+    return inject.energy_angle_sampler(p, lambda r, k: np.full(k, 100.0), inject.gaussian_angle(2.0))
+
+
+def test_oracle_batch_loop_matches_reference_cfg1_full_run():
+    """80x200 floating conductive mask, 10k ions + 10k electrons per batch, 30 batches:
+    the oracle batch loop reproduces the reference run() bit for bit."""
+    g = load_golden("run_cfg1_30.npz")
+    p = g["p"]
+    solid, mask, _, _ = geometry.build_geometry(p)
+    np.testing.assert_array_equal(solid, g["solid"])
+    st = OF.BatchState(p, solid, mask)
+    rng = np.random.default_rng(p.seed)
+    samp = cfg1_ion_sampler(p)
+    for _ in range(p.n_batches):
+        parts = inject.inject(p, p.n_per_batch, solid.shape[1], rng, None, samp)
+        st.step(*OT.trace(*parts, st.Ex, st.Ey, ~solid, p, st.barrier()))
+    np.testing.assert_array_equal(st.rho, g["rho_raw"])
+    np.testing.assert_allclose(st.phi, g["mean_phi"], rtol=0, atol=1e-12)
+    for k in st.hist:
+        np.testing.assert_array_equal(np.array(st.hist[k]), g[f"hist_{k}"])
+
+
 @pytest.mark.parametrize("name", ["floating", "fixed", "dielectric", "cfg2"])
 def test_oracle_fields_match_reference(name):
     g = load_golden(f"fields_{name}.npz")

@@ -127,6 +127,45 @@ def test_fp32_batch_loop_tracks_oracle(case_cls):
     assert np.max(np.abs(res["mean_phi"] - st.phi)) <= 0.01 * swing
 
 
+def _cfg1_sampler(p):
+    return inject.energy_angle_sampler(p, lambda r, k: np.full(k, 100.0), inject.gaussian_angle(2.0))
+
+
+def test_fp64_batch_loop_matches_reference_cfg1_full_run(case_cls):
+    """80x200 floating conductive mask, DC 100 eV ions at N(0, 2 deg), 10k + 10k per
+    batch, 30 batches: FP64 tracer + FP64 Green's operator reproduce the reference
+    run() (1e-10 relative on charge and potential, exact counts)."""
+    g = load_golden("run_cfg1_30.npz")
+    p = g["p"]
+    case = case_cls(p, precision="f64", green="f64")
+    res = case.run(ion_velocity=_cfg1_sampler(p))
+    np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(res["mean_phi"], g["mean_phi"], rtol=1e-10, atol=1e-8)
+    for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
+        np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])
+    np.testing.assert_allclose(res["hist"]["leak"], g["hist_leak"], rtol=1e-9, atol=1e-12)
+
+
+def test_fp32_batch_loop_tracks_reference_cfg1_full_run(case_cls):
+    """Same 30-batch run with the FP32 tracer: per-batch bottom ion flux within
+    3 sigma of the reference (counting noise of the batch), the final surface
+    charge's total within 1%, and the potential within 1e-3 V of the reference
+    wherever the two runs deposited the same charge history up to noise (max error
+    over the grid within 2% of the potential swing)."""
+    g = load_golden("run_cfg1_30.npz")
+    p = g["p"]
+    case = case_cls(p, precision="f32", green="f64")
+    res = case.run(ion_velocity=_cfg1_sampler(p))
+    ri, ro = res["hist"]["ratio_i_bottom"], g["hist_ratio_i_bottom"]
+    norm = p.n_per_batch * (case.b1 - case.b0) / p.nx
+    sigma = np.sqrt(np.maximum(ro * norm, 1)) / norm
+    assert np.all(np.abs(ri - ro) <= 3 * sigma + 1e-12), (ri, ro)
+    tot_ref, tot = g["rho_raw"].sum(), res["rho_raw"].sum()
+    assert abs(tot - tot_ref) <= 0.01 * abs(g["rho_raw"]).sum()
+    swing = np.ptp(g["mean_phi"])
+    assert np.max(np.abs(res["mean_phi"] - g["mean_phi"])) <= 0.02 * swing
+
+
 def test_graph_replay_equals_eager(case_cls):
     """A captured batch replays the same kernels: same counts as an eager batch."""
     import torch
