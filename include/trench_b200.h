@@ -204,6 +204,8 @@ typedef struct {
     int angle_random_sign;           /* draw the sign of the angle with probability 1/2 */
     const int32_t *d_counter;        /* optional device batch counter: the Philox batch word is
                                         batch + *d_counter + 1 (lets a CUDA graph replay a new batch) */
+    uint16_t *d_bin_e, *d_bin_a;     /* optional (n_species): table bin of each ion's energy / angle
+                                        (0 when that quantity has no table); the adjoint's histories */
 } tb_inject_args;
 
 int tb_inject(tb_ctx *ctx, const tb_inject_args *args, void *stream);
@@ -248,6 +250,68 @@ int tb_pack_check(tb_pack *pack, void *stream);
 #define TB_NOALLOC_MAX_CELLS 65536
 int tb_trace_f32_noalloc(int nx, int ny, double dx, const uint8_t *d_vac, const tb_trace_args *args,
                          double vscale, void *stream);
+
+/* ---- Adjoint of the charging loop -----------------------------------------------
+ * No counterpart in the reference, which has no gradient.  The gradient of a
+ * charging objective with respect to the ion energy/angle histogram weights and the
+ * surface charge is taken by likelihood-ratio reweighting of the traced histories:
+ * per batch b the absorbed ions are tallied by (table bin, surface slot), so that a
+ * change of the bin probabilities by factors rE[k], rA[l] changes the expected ion
+ * deposit on slot s to
+ *     ci_b[s](r) = Ni_b[s] + sum_k (rE[k] - 1) TE_b[k][s] + sum_l (rA[l] - 1) TA_b[l][s]
+ * (Ni_b = the traced count; first order in r - 1, exact at r = 1).  The charge
+ * update of tb_step_charge then runs over these deposits -- the surrogate recurrence,
+ * traced histories held fixed -- and its adjoint is swept backwards, optionally with
+ * the deposits' measured response to the charge state (field feedback) added. */
+
+/* Tally one traced batch.  Ions are particles [0, n_species), electrons
+ * [n_species, 2 n_species).  An absorbed particle (status 1) on cell c adds 1 in
+ * column d_slot[c] of the table, (n_energy + n_angle + 2, m) int32, accumulated:
+ * an ion to rows bin_e, n_energy + bin_a and n_energy + n_angle (all ions), an
+ * electron to row n_energy + n_angle + 1.  A bin index out of range, or an absorbed
+ * particle off the surface, raises the context's device check flag (tb_check). */
+typedef struct {
+    int64_t n_species;
+    const int8_t *d_status;          /* (2 n_species) */
+    const int32_t *d_hit;            /* (2 n_species) absorbing cell */
+    const uint16_t *d_bin_e, *d_bin_a; /* (n_species) */
+    const int32_t *d_slot;           /* (nx*ny) surface slot of each cell or -1 */
+    int m, n_energy, n_angle;
+    int32_t *d_table;
+} tb_tally_args;
+int tb_tally(tb_ctx *ctx, const tb_tally_args *args, void *stream);
+
+/* The surrogate recurrence over n_batches stored tables (consecutive, each
+ * (n_energy + n_angle + 2, m)).  The charge-update fields of the step descriptor
+ * are used (m, d_sflag, d_leak_M, d_leak_h, d_g_s, c_slot, floating, driven,
+ * q_macro, dx, C_cond, Te) together with its scratch d_rho_prev (m) and d_work (2m). */
+typedef struct {
+    int n_batches, n_energy, n_angle;
+    const int32_t *d_tables;
+    const double *d_rE, *d_rA;       /* (n_energy), (n_angle) reweighting factors; NULL = 1 */
+    const double *d_leak_MT;         /* (m, m) transpose of the leakage operator (reverse sweep) */
+    double *d_rho;                   /* (m) state: in before the first batch, out after the last */
+    double *d_scal;                  /* (n_batches, 4) per batch: ion and electron deposit on the
+                                        floating conductor, drift (written forward, read reverse) */
+    double *d_bottom;                /* (n_batches) reweighted ion deposit on the bottom slots */
+    /* Field feedback (reverse sweep only; n_basis = 0 leaves it out): the deposits'
+       linear response to the charge state, measured in a basis of n_basis surface-charge
+       modes.  d_basis (m, n_basis) orthonormal columns; d_resp_i, d_resp_e (n_sets, m,
+       n_basis): ion / electron deposit per unit charge along each mode; d_resp_index
+       (n_batches): the response set of each batch, or -1. */
+    int n_basis;
+    const double *d_basis, *d_resp_i, *d_resp_e;
+    const int32_t *d_resp_index;
+} tb_adjoint_args;
+/* Forward: rho <- recurrence(rho) over the batches; writes d_scal and d_bottom. */
+int tb_adjoint_forward(tb_ctx *ctx, const tb_step_desc *step, const tb_adjoint_args *args, void *stream);
+/* Reverse over the same batches (their d_scal from the forward):
+ *   d_lambda (m): in dJ/d rho after the last batch, out dJ/d rho before the first;
+ *   d_gbottom (n_batches): dJ/d bottom deposit of each batch (NULL = 0);
+ *   d_grad (n_energy + n_angle): accumulates dJ/d rE, dJ/d rA.
+ * Needs the descriptor's d_work (2m) and 2m + 4 + n_basis doubles in d_scratch. */
+int tb_adjoint_reverse(tb_ctx *ctx, const tb_step_desc *step, const tb_adjoint_args *args, double *d_lambda,
+                       const double *d_gbottom, double *d_grad, double *d_scratch, void *stream);
 
 /* Measured shared-memory load bandwidth of the context's GPU (GB/s, all SMs, 8-byte
  * loads like the FP32 tracer's gathers).  A benchmark helper; synchronises the device. */

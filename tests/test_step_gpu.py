@@ -134,12 +134,13 @@ def _cfg1_sampler(p):
 def test_fp64_batch_loop_matches_reference_cfg1_full_run(case_cls):
     """80x200 floating conductive mask, DC 100 eV ions at N(0, 2 deg), 10k + 10k per
     batch, 30 batches: FP64 tracer + FP64 Green's operator reproduce the reference
-    run() (1e-10 relative on charge and potential, exact counts)."""
+    run() (1e-10 relative on charge and potential, exact counts).  The absolute floor
+    scales with the largest charge (1.9e7 C/m^3): leakage spreads tails down to 1e-8."""
     g = load_golden("run_cfg1_30.npz")
     p = g["p"]
     case = case_cls(p, precision="f64", green="f64")
     res = case.run(ion_velocity=_cfg1_sampler(p))
-    np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-13 * np.abs(g["rho_raw"]).max())
     np.testing.assert_allclose(res["mean_phi"], g["mean_phi"], rtol=1e-10, atol=1e-8)
     for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
         np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])

@@ -92,6 +92,28 @@ class InjectArgs(ctypes.Structure):
         ("n_angle", ctypes.c_int),
         ("angle_random_sign", ctypes.c_int),
         ("d_counter", _vp),
+        ("d_bin_e", _vp), ("d_bin_a", _vp),
+    ]
+
+
+class TallyArgs(ctypes.Structure):
+    """Mirror of ``tb_tally_args``."""
+    _fields_ = [
+        ("n_species", _i64),
+        ("d_status", _vp), ("d_hit", _vp), ("d_bin_e", _vp), ("d_bin_a", _vp), ("d_slot", _vp),
+        ("m", ctypes.c_int), ("n_energy", ctypes.c_int), ("n_angle", ctypes.c_int),
+        ("d_table", _vp),
+    ]
+
+
+class AdjointArgs(ctypes.Structure):
+    """Mirror of ``tb_adjoint_args``."""
+    _fields_ = [
+        ("n_batches", ctypes.c_int), ("n_energy", ctypes.c_int), ("n_angle", ctypes.c_int),
+        ("d_tables", _vp), ("d_rE", _vp), ("d_rA", _vp), ("d_leak_MT", _vp),
+        ("d_rho", _vp), ("d_scal", _vp), ("d_bottom", _vp),
+        ("n_basis", ctypes.c_int),
+        ("d_basis", _vp), ("d_resp_i", _vp), ("d_resp_e", _vp), ("d_resp_index", _vp),
     ]
 
 
@@ -124,6 +146,10 @@ SIGNATURES = {
     "tb_pack_set_args": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs)]),
     "tb_pack_trace": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "tb_pack_check": (ctypes.c_int, [_vp, _vp]),
+    "tb_tally": (ctypes.c_int, [_vp, ctypes.POINTER(TallyArgs), _vp]),
+    "tb_adjoint_forward": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), ctypes.POINTER(AdjointArgs), _vp]),
+    "tb_adjoint_reverse": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), ctypes.POINTER(AdjointArgs), _vp, _vp,
+                                          _vp, _vp, _vp]),
     "tb_trace_f32_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _dbl, _vp, ctypes.POINTER(TraceArgs),
                                             _dbl, _vp]),
 }

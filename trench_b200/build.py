@@ -26,6 +26,7 @@ UNITS = {
     "tb_step.cu": ["-fmad=false"],
     "tb_bench.cu": [],
     "tb_inject.cu": [],
+    "tb_adjoint.cu": ["-fmad=false"],
 }
 
 

@@ -39,13 +39,15 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k
 __device__ __forceinline__ double unit(uint32_t r) { return ((double)r + 0.5) * 2.3283064365386963e-10; }
 
 // Inverse CDF of a histogram: cdf[0..nb] increasing from 0 to 1 over bin edges
-// edges[0..nb]; linear within a bin.
-__device__ double sample_table(const double *edges, const double *cdf, int nb, double u) {
+// edges[0..nb]; linear within a bin.  *bin receives the bin drawn (a bin of zero
+// weight is never drawn: the search ends on cdf[lo] <= u < cdf[lo + 1]).
+__device__ double sample_table(const double *edges, const double *cdf, int nb, double u, int *bin) {
     int lo = 0, hi = nb;  // cdf[lo] <= u < cdf[hi]
     while (hi - lo > 1) {
         const int mid = (lo + hi) >> 1;
         if (cdf[mid] <= u) lo = mid; else hi = mid;
     }
+    *bin = lo;
     const double w = cdf[hi] - cdf[lo];
     const double f = w > 0 ? (u - cdf[lo]) / w : 0.5;
     return edges[lo] + f * (edges[hi] - edges[lo]);
@@ -62,11 +64,13 @@ __global__ void k_inject(const tb_inject_args a) {
     double x = u0 * a.lx, vx, vy, qm;
     int8_t spc;
     if (i < n) {
-        const double e = a.n_energy > 0 ? sample_table(a.d_energy_edges, a.d_energy_cdf, a.n_energy, u1)
+        int be = 0, ba = 0;
+        const double e = a.n_energy > 0 ? sample_table(a.d_energy_edges, a.d_energy_cdf, a.n_energy, u1, &be)
                                         : a.ion_energy_eV;
+        if (a.d_bin_e) a.d_bin_e[i] = (uint16_t)be;
         const double v = sqrt(2.0 * fmax(e, 0.0) * a.e_charge / a.ion_mass);
         if (a.n_angle > 0) {
-            double th = sample_table(a.d_angle_edges, a.d_angle_cdf, a.n_angle, u2);
+            double th = sample_table(a.d_angle_edges, a.d_angle_cdf, a.n_angle, u2, &ba);
             if (a.angle_random_sign && u3 < 0.5) th = -th;
             vx = v * sin(th);
             vy = -v * cos(th);
@@ -75,6 +79,7 @@ __global__ void k_inject(const tb_inject_args a) {
             vx = a.ion_lateral_sigma * sqrt(-2.0 * log(u2)) * cos(6.283185307179586 * u3);
             vy = -v;
         }
+        if (a.d_bin_a) a.d_bin_a[i] = (uint16_t)ba;
         qm = a.qm_ion;
         spc = 0;
     } else {
@@ -110,6 +115,8 @@ extern "C" int tb_inject(tb_ctx *ctx, const tb_inject_args *a, void *stream) {
     if ((a->n_energy > 0 && (!a->d_energy_edges || !a->d_energy_cdf)) ||
         (a->n_angle > 0 && (!a->d_angle_edges || !a->d_angle_cdf)))
         return tb_fail(ctx, TB_ERR_ARG, "tb_inject: a sampling table is missing");
+    if (a->n_energy > 65536 || a->n_angle > 65536)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_inject: a table has more than 65536 bins");
     if (a->n_species == 0) return TB_OK;
     TB_CUDA(ctx, cudaSetDevice(ctx->device));
     const long long total = 2 * a->n_species;

@@ -155,7 +155,7 @@ class DeviceInjector:
     (energy in eV, angle in radians); None uses p.ion_energy_eV / the lateral
     thermal velocity of p.ion_temp_eV like the reference."""
 
-    def __init__(self, case, seed=0, energy_table=None, angle_table=None, angle_random_sign=True):
+    def __init__(self, case, seed=0, energy_table=None, angle_table=None, angle_random_sign=True, bins=False):
         import ctypes
         import torch
         from . import _capi
@@ -188,6 +188,12 @@ class DeviceInjector:
             self._keep += [e, c]
             a.d_angle_edges, a.d_angle_cdf, a.n_angle = _ptr(e), _ptr(c), len(angle_table[0]) - 1
         a.angle_random_sign = int(bool(angle_random_sign))
+        self.bin_e = self.bin_a = None
+        if bins:
+            # table bin of every ion's energy and angle (the adjoint's histories)
+            self.bin_e = torch.zeros(int(p.n_per_batch), dtype=torch.uint16, device=dev)
+            self.bin_a = torch.zeros(int(p.n_per_batch), dtype=torch.uint16, device=dev)
+            a.d_bin_e, a.d_bin_a = _ptr(self.bin_e), _ptr(self.bin_a)
         self.args = a
         self._ctypes = ctypes
         self._capi = _capi

@@ -160,6 +160,8 @@ class ChargingCase:
             self._args = _capi.TraceArgs()
             self._graph = None
             self.trace_events = None   # optional (start, end) CUDA events around the tracer launch
+            self.hit = None            # optional (capacity,) int32: absorbing cell of each particle
+            self.after_trace = None    # optional callable run on the stream between trace and charge update
             self.rf = None
             if p.field_mode == "circuit_rf":
                 self._build_rf(circuit, solver, eps, cond, vac)
@@ -314,7 +316,7 @@ class ChargingCase:
         a.tapered = int(is_tapered(p))
         a.d_counts, a.d_totals = _ptr(self.counts), _ptr(self.totals)
         a.d_status, a.d_steps = _ptr(self.status), _ptr(self.steps)
-        a.d_hit = None
+        a.d_hit = _ptr(self.hit) if self.hit is not None else None
         a.write_state = 0
         precision = self.precision
         if self.rf is not None:
@@ -347,6 +349,8 @@ class ChargingCase:
             self.ctx.check(L.tb_trace(self.ctx.handle, ctypes.byref(a), _capi.PRECISION[precision], s))
         if ev is not None:
             ev[1].record()
+        if self.after_trace is not None:
+            self.after_trace()
         self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
         self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
 
@@ -354,8 +358,8 @@ class ChargingCase:
 
     def autotune_tracer(self, n=None, reps=2):
         """Times the tracer's launch shapes (CTA size, CTAs per SM) on the loaded batch and
-        keeps the fastest.  Traces only: the charge state is not changed (the trace is
-        deterministic, so every shape gives the same counts)."""
+        keeps the fastest.  Traces only: neither the charge state nor the loaded batch is
+        changed (the trace is deterministic, so every shape gives the same counts)."""
         L = _capi.lib()
         n = self.n_loaded if n is None else n
         p = self.p
@@ -381,20 +385,29 @@ class ChargingCase:
         return timings
 
     def _trace_only(self, n):
-        """The tracer launch of step() alone (counts and status are overwritten by the next step)."""
+        """The tracer launch of step() alone (counts and status are overwritten by the next step).
+        The tracer writes the state of particles still live at the step cap back to its
+        inputs, so the launch traces a copy of the loaded batch (in the second input
+        buffer set) and leaves the batch itself as it was."""
         L = _capi.lib()
         s = self._stream()
+        X1, S1 = self.add_input_buffer()
+        for dst, src in zip(X1 + [S1], self.X + [self.SPC]):
+            dst[:n].copy_(src[:n])
         self.status[:n].fill_(3)
         self.steps[:n].zero_()
         self.counts.zero_()
         self.totals.zero_()
-        precision = self._fill_args(n)
+        precision = self._fill_args(n, 1)
+        clock = self.clock[:n].clone() if self.rf is not None else None   # in/out RF launch clocks
         ev = self.trace_events
         if ev is not None:
             ev[0].record()
         self.ctx.check(L.tb_trace(self.ctx.handle, ctypes.byref(self._args), _capi.PRECISION[precision], s))
         if ev is not None:
             ev[1].record()
+        if clock is not None:
+            self.clock[:n].copy_(clock)
 
     def capture(self, n=None, buffer=0):
         """Capture one batch (for n particles in input buffer set `buffer`) as a CUDA graph."""
