@@ -314,6 +314,7 @@ def run_b200(args, p):
             dist.barrier()
             dist.destroy_process_group()
         return 0
+    adj = adjoint_measure() if (args.adjoint and world == 1) else None
 
     particles = n * args.steps * world
     value = particles / (total_ms / 1000.0)
@@ -348,6 +349,7 @@ def run_b200(args, p):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "batches_per_s": 1000.0 * args.steps * world / e2e_total},
             "device_injection": dinj,
+            "adjoint": adj,
             "gpu_launches": 10 * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "wall_s": wall}
@@ -446,6 +448,63 @@ def device_injection(case, p, steps):
                     "history row read back each step"}
 
 
+def adjoint_measure():
+    """The adjoint on the AR-5 sensitivity workload (2^20 ions + 2^20 electrons per batch,
+    50 batches, 64-bin IED, 32-bin IAD): recording time of the forward run (with 32
+    field-feedback modes every 5 batches), backward time of each objective, and the
+    directional derivative along +-10% on the 140 eV peak's bins against central
+    differences of the full charging chain on the same Philox draws."""
+    import time
+    import torch
+    from trench_b200 import adjoint, inject
+    from trench_b200.step import ChargingCase
+    p, eE, wE, eA, wA = adjoint.adjoint_workload()
+    B = p.n_batches
+    case = ChargingCase(p, precision="f32", max_batches=B)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = adjoint.AdjointRecorder(case, eE, wE, eA, wA, seed=21).run(B)
+    torch.cuda.synchronize()
+    record_s = time.perf_counter() - t0
+    cE = 0.5 * (eE[1:] + eE[:-1])
+    vE = np.where(np.abs(cE - 140) < 15, 1.0, 0.0)
+    out = {"workload": "AR-5 trench 20x100 cells (60x180 grid), floating conductive mask; 64-bin IED 0-300 eV, "
+                       "32-bin IAD 0-10 deg; 2^20 ions + 2^20 electrons per batch; 50 batches; "
+                       "histories checkpointed every 10 batches; 32 feedback modes every 5 batches",
+           "record_s": record_s, "record_particles_per_s": 2 * p.n_per_batch * B / record_s}
+    f64 = torch.float64
+    for name in ("phi_bottom", "ratio_i_bottom"):
+        for fb in (True, False):
+            gE = torch.tensor(wE, dtype=f64, device=case.dev, requires_grad=True)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            o = adjoint.objectives(hist, gE, None, feedback=fb)
+            J = o[name] if name == "phi_bottom" else o[name][-1]
+            J.backward()
+            torch.cuda.synchronize()
+            key = name + ("" if fb else "_frozen")
+            out[f"backward_s_{key}"] = time.perf_counter() - t0
+            out[f"d_{key}"] = float(np.dot(gE.grad.cpu().numpy(), wE * vE))
+
+    def chain(w):
+        c = ChargingCase(p, precision="f32", max_batches=B)
+        inj = inject.DeviceInjector(c, 21, energy_table=inject.histogram_table(eE, w),
+                                    angle_table=inject.histogram_table(eA, wA))
+        for _ in range(B):
+            inj()
+            c.step()
+        h = c.history()
+        return np.array([h["bottom center"][-1], h["ratio_i_bottom"][-1]])
+
+    fd = (chain(wE * (1 + 0.1 * vE)) - chain(wE * (1 - 0.1 * vE))) / 0.2
+    out["chain_fd"] = {"phi_bottom": float(fd[0]), "ratio_i_bottom": float(fd[1]),
+                       "direction": "bins within 15 eV of 140 eV scaled by 1 +- 0.1, same seed"}
+    for key, ref in (("phi_bottom", fd[0]), ("ratio_i_bottom", fd[1])):
+        out[f"rel_err_{key}"] = abs(out[f"d_{key}"] - ref) / abs(ref)
+        out[f"rel_err_{key}_frozen"] = abs(out[f"d_{key}_frozen"] - ref) / abs(ref)
+    return out
+
+
 def case_smem_peak(case):
     """Shared-memory load bandwidth measured on this GPU (GB/s)."""
     import ctypes
@@ -466,6 +525,8 @@ def main():
     ap.add_argument("--workload", default="ar8", choices=["ar8", "sweep"],
                     help="ar8: the AR-8 RF-charging case (default); sweep: many uneven cases per launch")
     ap.add_argument("--cases", type=int, default=64, help="cases of the sweep workload")
+    ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
+                    help="skip the adjoint measurement (AR-5 sensitivity workload, 1 GPU only)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
