@@ -48,6 +48,30 @@ def test_solver_matches_reference_lu(case_cls, name):
         assert case.C_cond == pytest.approx(float(g["C_cond"]), rel=1e-9)
 
 
+@pytest.mark.parametrize("shape", ["large_dielectric", "medium_floating"])
+def test_solver_matches_reference_lu_on_large_grids(cuda_device, shape):
+    """The 400x1400 fine-grid geometry (560,000 cells, dielectric mask) and a 200x700
+    floating conductive mask: multigrid (residual target 5e-16 sqrt(n)) against the
+    oracle's sparse LU (the reference's solver) for the external potential and a random
+    surface charge of tens of volts, within 1e-6 V."""
+    from trench_b200.fields import setup_fields
+    if shape == "large_dielectric":
+        p = replace(Params(), dx=1.25e-9, nx=400, trench_w=40, trench_d=800, floor_t=20, mask_t=80, n_vac=500,
+                    mask_type="dielectric", bias="dc", field_mode="floating")
+    else:
+        p = replace(Params(), dx=2.5e-9, nx=200, trench_w=40, trench_d=400, floor_t=20, mask_t=80, n_vac=200,
+                    mask_type="conductor", bias="dc", field_mode="floating")
+    solid, mask, _, _ = geometry.build_geometry(p)
+    want = OF.setup_fields(p, solid, mask)
+    got = setup_fields(p, solid, mask, device=cuda_device)
+    np.testing.assert_allclose(got["external"], want["external"], rtol=0, atol=1e-6)
+    rho = np.where(OF.surface_cells(solid), np.random.default_rng(2).normal(size=solid.shape), 0.0) * 1e7
+    b = (-rho / EPS0).ravel()
+    ref = want["solve"](b)
+    assert np.abs(ref).max() > 1.0
+    np.testing.assert_allclose(got["solve"](b), ref, rtol=0, atol=1e-6)
+
+
 @pytest.mark.parametrize("name", ["floating", "dielectric", "cfg2"])
 def test_green_operator_reproduces_solve(case_cls, name):
     """phi = external + G rho_s on every row cell, for an arbitrary surface charge."""

@@ -133,6 +133,42 @@ def test_f32_large_sample_agreement_and_bottom_flux(tracers):
     assert agree >= 0.999, f"hit agreement {agree:.5f}"
 
 
+def test_global_memory_path_on_a_large_grid(tracers):
+    """A 200x700 grid (2.5 nm cells, AR-10 trench 40 x 400 cells, dielectric mask 80):
+    the packed FP32 field (1.1 MB) exceeds shared memory, so the FP32 tracer reads it
+    through L2.  Fields: external plus a random surface charge scaled to 20 V.  FP64
+    kernel: status, absorbing cell and step count equal the oracle per particle; FP32:
+    hit cells agree for >= 99.9% and the bottom ion flux is within 3 sigma."""
+    from oracle import oracle_fields as OF
+    p = replace(Params(), dx=2.5e-9, nx=200, trench_w=40, trench_d=400, floor_t=20, mask_t=80, n_vac=200,
+                mask_type="dielectric", max_steps=8000, electron_temp_eV=3.0)
+    solid, mask, _, _ = geometry.build_geometry(p)
+    assert (solid.shape[0] + 2) * (solid.shape[1] + 2) * 8 > 227 * 1024
+    f = OF.setup_fields(p, solid, mask)
+    rng = np.random.default_rng(5)
+    rho = np.where(OF.surface_cells(solid), rng.normal(size=solid.shape), 0.0)
+    phi1 = f["solve"]((-rho / OF.EPS0).ravel()).reshape(solid.shape)
+    phi = f["external"] + phi1 * (20.0 / np.abs(phi1).max())
+    Ex, Ey = OF.compute_field(phi, ~solid, p, f["volts"]["top"])
+    bar = (phi, np.where(f["cond"], 1.0, f["eps"] / (1.0 + f["eps"])))
+    n = 1 << 14
+    sampler = inject.energy_angle_sampler(p, lambda r, k: np.full(k, 100.0), inject.half_gaussian_angle(6.0))
+    x, y, vx, vy, qm, spc = inject.inject(p, n, solid.shape[1], rng, ion_velocity=sampler)
+    want = OT.trace_detail(x, y, vx, vy, qm, Ex, Ey, ~solid, p, bar)
+    t64 = tracers(solid, "f64")
+    t64(x, y, vx, vy, qm, spc, Ex, Ey, ~solid, p, bar)
+    for k in ("status", "hit", "steps"):
+        np.testing.assert_array_equal(t64.last[k], want[k])
+    t32 = tracers(solid, "f32")
+    got = t32(x, y, vx, vy, qm, spc, Ex, Ey, ~solid, p, bar)
+    same = (t32.last["status"] == want["status"]) & (t32.last["hit"] == want["hit"])
+    assert same.mean() >= 0.999, f"hit agreement {same.mean():.5f}"
+    ref = OT.counts_from_detail(want, spc, solid.shape)
+    b0, b1 = geometry.opening_span(solid, p.floor_t)
+    a, r = got[0][b0:b1, p.floor_t - 1].sum(), ref[0][b0:b1, p.floor_t - 1].sum()
+    assert abs(a - r) <= 3 * np.sqrt(max(r, 1)), (a, r)
+
+
 def test_empty_launch(tracers):
     p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12)
     solid, _, _, _ = geometry.build_geometry(p)

@@ -42,6 +42,7 @@ struct K32 {
     unsigned long long *queue;
     int *err;
     int bytes;                      // packed field bytes (multiple of 16)
+    int pool_off;                   // byte offset of the drain pool in dynamic shared memory, -1 = none
 };
 
 // 1.0f for a vacuum cell, 0.0f for a solid one, with integer operations only
@@ -100,45 +101,235 @@ __device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mba
     return __syncthreads_and(done) != 0;
 }
 
-// Traces particles of one case with the calling warp until the case's queue is
-// drained and every lane of the warp is empty, then adds the warp's tallies to the
-// case's totals.  `fieldp` is the packed field in shared or global memory.
+// One lane's particle: cell (ix, iy) and FP32 offset (ox, oy) in [0,1) cell units,
+// velocity in vscale units; pid < 0 = no particle.
+struct LaneState {
+    int pid, ix, iy, steps, stop_at, spc;
+    float ox, oy, vx, vy, qm;
+};
+
+// Per-lane event counts, reduced over the warp at the end.
+struct LaneTally {
+    unsigned steps, esc_i, esc_e, lost, hit_i, hit_e;
+};
+
+// Loop-invariant parameters of one case.
 template <bool SMEM>
-__device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp) {
+struct CaseView {
+    FieldView<SMEM> F;
+    int nx, ny, cells, P;
+    float inv_v, cfl;
+    bool barrier, tapered, first_face;
+};
+
+// One step of one particle (trench_charging_2d.py:584-650): vacuum-weighted bilinear
+// field, CFL step, trapezoid update, periodic x, escape, staircase corner, first-face
+// wall entry and barrier reflection; on absorption, escape or the step cap the
+// particle's outputs are written and s.pid becomes -1.
+template <bool SMEM>
+__device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM> &C, LaneState &s, LaneTally &t) {
+    const tb_trace_args &a = k.a;
+    const int nx = C.nx, ny = C.ny, P = C.P;
+    // ---- vacuum-weighted bilinear field (trench_charging_2d.py:492-509) ----
+    // corners (i0, j0) = (ix - 1 + hx, iy - 1 + hy) .. (i0 + 1, j0 + 1); in the halo-padded
+    // field i0 + 1 = ix + hx needs no wrap and the clipped rows need one clamp
+    const int hx = s.ox >= 0.5f ? 1 : 0, hy = s.oy >= 0.5f ? 1 : 0;
+    const float tx = hx ? s.ox - 0.5f : s.ox + 0.5f;
+    const float ty = hy ? s.oy - 0.5f : s.oy + 0.5f;
+    const int base = (s.ix + hx) * P + max(s.iy + hy, 0);
+    const tb_fcell c00 = C.F.at(base), c01 = C.F.at(base + 1);
+    const tb_fcell c10 = C.F.at(base + P), c11 = C.F.at(base + P + 1);
+    const float ux = 1.f - tx, uy = 1.f - ty;
+    const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
+    const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
+    const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
+    const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
+    const float qs = __fdividef(s.qm, fmaxf(sw, 1e-12f));
+    const float ax = qs * sex, ay = qs * sey;
+    // the start cell is the corner on the particle's side of each centre line; its
+    // interior flag says every 8-neighbour is vacuum, so a move of < 1 cell cannot
+    // touch a wall and the end-cell and corner checks are skipped
+    const float start_ey = hx ? (hy ? c00.ey : c01.ey) : (hy ? c10.ey : c11.ey);
+    const bool near = !(__float_as_uint(start_ey) & 1u);
+
+    // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
+    const float speed = sqrtf(s.vx * s.vx + s.vy * s.vy);
+    const float acc = sqrtf(ax * ax + ay * ay);
+    const float dt = __fdividef(C.cfl, speed + sqrtf(2.f * acc) + C.inv_v);
+    const float vxn = s.vx + ax * dt, vyn = s.vy + ay * dt;
+    const float sx = 0.5f * (s.vx + vxn) * dt, sy = 0.5f * (s.vy + vyn) * dt;
+    float nox = s.ox + sx, noy = s.oy + sy;
+    const bool gx = nox >= 1.f, lx = nox < 0.f, gy = noy >= 1.f, ly = noy < 0.f;
+    const int dix = gx ? 1 : (lx ? -1 : 0);
+    const int diy = gy ? 1 : (ly ? -1 : 0);
+    nox = fminf(gx ? nox - 1.f : (lx ? nox + 1.f : nox), ONE_BELOW);
+    noy = fminf(gy ? noy - 1.f : (ly ? noy + 1.f : noy), ONE_BELOW);
+    int nix = s.ix + dix;
+    nix = nix < 0 ? nx - 1 : (nix >= nx ? 0 : nix);
+    const int niy = s.iy + diy;
+    ++s.steps;
+    ++t.steps;
+    const bool escaped = niy >= ny;
+    bool hit_end = false, corner = false;
+    if (near && !escaped) {
+        hit_end = !C.F.vac((nix + 1) * P + max(niy, -1) + 1);
+        // both the column and the (clipped) row changed: a staircase corner may lie on
+        // the path between two vacuum cells (trench_charging_2d.py:614-621)
+        corner = C.tapered && !hit_end && dix != 0 && max(niy, 0) != max(s.iy, 0);
+    }
+
+    if (!(hit_end || corner || escaped || s.steps >= s.stop_at)) {
+        s.ix = nix; s.iy = niy; s.ox = nox; s.oy = noy; s.vx = vxn; s.vy = vyn;
+        return;
+    }
+
+    // ---- rare path: wall contact, escape, or step cap ----
+    const int y0c = min(max(s.iy, 0), ny - 1);
+    const int iyn = min(max(niy, 0), ny - 1);
+    const int diy_e = iyn - y0c;     // rows clipped like the reference
+    bool hit = hit_end;
+    int dcell = nix * ny + iyn;
+    bool reflected = false;
+    if (hit ? C.first_face : corner) {
+        // first solid face crossed (trench_charging_2d.py:512-539) in cell units
+        const float inf = __int_as_float(0x7f800000);
+        const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - s.ox) / sx : inf;
+        const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - s.oy) / sy : inf;
+        const bool x_first = fx < fy;
+        const int ax_ = x_first ? nix : s.ix, ay_ = x_first ? y0c : y0c + diy_e;
+        const bool use_last = dix != 0 && diy_e != 0 && C.F.vac((ax_ + 1) * P + ay_ + 1);
+        const int cx = use_last ? nix : ax_, cy = use_last ? y0c + diy_e : ay_;
+        const bool face_x = use_last ? !x_first : x_first;
+        const int ccell = cx * ny + cy;
+        hit = !C.F.vac((cx + 1) * P + cy + 1);
+        dcell = ccell;
+        if (hit && C.barrier) {
+            const float4 b = __ldg(k.barrier + ccell);
+            // neighbour the particle came from: W/E across an x face, S/N across a y face
+            const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
+            const float vn = face_x ? vxn : vyn;
+            if (0.5f * vn * vn < s.qm * dphi) {
+                // reflect: the normal velocity flips, the position stays at the start point
+                s.vx = face_x ? -vxn : vxn;
+                s.vy = face_x ? vyn : -vyn;
+                hit = false;
+                reflected = true;
+            }
+        }
+    }
+    if (!reflected) { s.ix = nix; s.iy = niy; s.ox = nox; s.oy = noy; s.vx = vxn; s.vy = vyn; }
+
+    int done = 0;
+    if (hit) {
+        if (dcell < 0 || dcell >= C.cells) {
+            atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BAD_CELL);
+        } else {
+            atomicAdd(a.d_counts + (size_t)s.spc * C.cells + dcell, 1);
+        }
+        if (a.d_hit) a.d_hit[s.pid] = dcell;
+        if (s.spc == 0) ++t.hit_i; else ++t.hit_e;
+        done = 1;
+    } else if (escaped && !reflected) {
+        if (s.spc == 0) ++t.esc_i; else ++t.esc_e;
+        done = 2;
+    } else if (s.steps >= s.stop_at) {
+        if (s.steps >= a.max_steps) ++t.lost;
+        done = 3;
+    }
+    if (done) {
+        const int pid = s.pid;
+        a.d_steps[pid] = s.steps;
+        if (done != 3) a.d_status[pid] = (int8_t)done;
+        if (done == 3 || a.write_state) {
+            a.d_x[pid] = ((double)s.ix + (double)s.ox) * k.dx;
+            a.d_y[pid] = ((double)s.iy + (double)s.oy) * k.dx;
+            a.d_vx[pid] = (double)s.vx * k.vscale;
+            a.d_vy[pid] = (double)s.vy * k.vscale;
+        }
+        s.pid = -1;
+    }
+}
+
+// Shared-memory pool of particle states for the drain of a case: 9 words per lane
+// (struct of arrays over the block's threads): pid; ix | iy << 16 (grids below 32768
+// cells a side, iy >= -1); steps; stop_at | spc << 31; ox, oy, vx, vy, qm.
+constexpr int POOL_WORDS = 9;
+constexpr int TAIL_ROUND_STEPS = 32;
+
+__device__ __forceinline__ void pool_put(uint32_t *P, int T, int q, const LaneState &s) {
+    P[0 * T + q] = (uint32_t)s.pid;
+    P[1 * T + q] = ((uint32_t)s.ix & 0xffffu) | ((uint32_t)s.iy << 16);
+    P[2 * T + q] = (uint32_t)s.steps;
+    P[3 * T + q] = (uint32_t)s.stop_at | ((uint32_t)s.spc << 31);
+    P[4 * T + q] = __float_as_uint(s.ox);
+    P[5 * T + q] = __float_as_uint(s.oy);
+    P[6 * T + q] = __float_as_uint(s.vx);
+    P[7 * T + q] = __float_as_uint(s.vy);
+    P[8 * T + q] = __float_as_uint(s.qm);
+}
+
+__device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneState &s) {
+    s.pid = (int)P[0 * T + q];
+    const uint32_t xy = P[1 * T + q];
+    s.ix = (int)(xy & 0xffffu);
+    s.iy = (int)xy >> 16;  // arithmetic shift keeps iy = -1
+    s.steps = (int)P[2 * T + q];
+    const uint32_t w = P[3 * T + q];
+    s.stop_at = (int)(w & 0x7fffffffu);
+    s.spc = (int)(w >> 31);
+    s.ox = __uint_as_float(P[4 * T + q]);
+    s.oy = __uint_as_float(P[5 * T + q]);
+    s.vx = __uint_as_float(P[6 * T + q]);
+    s.vy = __uint_as_float(P[7 * T + q]);
+    s.qm = __uint_as_float(P[8 * T + q]);
+}
+
+// Traces particles of one case with the calling block until the case's queue is
+// drained and every particle has ended, then adds the warps' tallies to the case's
+// totals.  `fieldp` is the packed field in shared or global memory.  Every thread of
+// the block calls it.
+//
+// Main phase: each lane takes a particle from the case's global queue whenever its
+// particle ends.  Drain: once the queue is empty a warp keeps only the lanes whose
+// particles are still in flight, so with independent warps the block would issue
+// nearly full instruction streams for a few live lanes each until the longest
+// particle ends.  With a shared-memory pool (pool != nullptr) the block instead runs
+// rounds: the live particles are packed into the first warps, those warps take up
+// to TAIL_ROUND_STEPS steps, and the rest wait at the barrier.  A particle's
+// arithmetic does not depend on its lane, so the results are the same either way.
+template <bool SMEM>
+__device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, uint32_t *pool) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const tb_trace_args &a = k.a;
-    const int nx = k.nx, ny = k.ny;
-    const int cells = nx * ny;
-    const int P = ny + 2;  // padded column stride
-    const float inv_v = k.inv_v;
-    const float4 *const barrier_tab = k.barrier;
-    int *const err = k.err;
     unsigned long long *const queue = k.queue;
 
-    FieldView<SMEM> F;
-    F.p = fieldp;
+    CaseView<SMEM> C;
+    C.F.p = fieldp;
+    C.nx = k.nx;
+    C.ny = k.ny;
+    C.cells = k.nx * k.ny;
+    C.P = k.ny + 2;  // padded column stride
+    C.inv_v = k.inv_v;
+    C.cfl = (float)a.cfl;
+    C.barrier = a.d_phi != nullptr;
+    C.tapered = a.tapered != 0;
+    C.first_face = C.barrier || C.tapered;
 
-    const float cfl = (float)a.cfl;
-    const bool barrier = a.d_phi != nullptr;
-    const bool tapered = a.tapered != 0;
-    const bool first_face = barrier || tapered;
-
-    // Particle state: cell (ix, iy) and FP32 offset (ox, oy) in [0,1) cell units.
-    // ix in [0, nx-1]; iy >= -1 in practice (below the grid only over a vacuum bottom row).
-    int pid = -1;
-    int ix = 0, iy = 0, steps = 0, stop_at = 0, spc = 0;
-    float ox = 0.f, oy = 0.f, vx = 0.f, vy = 0.f, qm = 0.f;
+    LaneState s;
+    s.pid = -1;
+    s.ix = s.iy = s.steps = s.stop_at = s.spc = 0;
+    s.ox = s.oy = s.vx = s.vy = s.qm = 0.f;
+    LaneTally t = {0u, 0u, 0u, 0u, 0u, 0u};
     bool open = true;
-    unsigned my_steps = 0, my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
 
     for (;;) {
         // One ballot per iteration: refill empty lanes from the global queue (one
-        // atomic per warp) or leave once the queue is drained and every lane is empty.
-        const unsigned need = __ballot_sync(FULL, pid < 0);
+        // atomic per warp) or leave once the queue is drained.
+        const unsigned need = __ballot_sync(FULL, s.pid < 0);
         if (need != 0u) {
             if (!open) {
-                if (need == FULL) break;
+                if (pool != nullptr || need == FULL) break;
             } else {
                 const int leader = __ffs(need) - 1;
                 const int cnt = __popc(need);
@@ -146,165 +337,74 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp) {
                 if (lane == leader) base = atomicAdd(queue, (unsigned long long)cnt);
                 base = __shfl_sync(FULL, base, leader);
                 if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
-                if (pid < 0) {
+                if (s.pid < 0) {
                     const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
                     if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
-                        pid = (int)idx;
+                        const int pid = (int)idx;
+                        s.pid = pid;
                         // metres -> cells: x lies in cell min(int(x/dx), nx-1) as in the
                         // reference (trench_charging_2d.py:611)
                         const double xc = a.d_x[pid] * k.inv_dx, yc = a.d_y[pid] * k.inv_dx;
-                        ix = min(max((int)xc, 0), nx - 1);
-                        iy = min((int)floor(yc), ny - 1);  // a start above the grid escapes at once
-                        ox = fminf(fmaxf((float)(xc - (double)ix), 0.f), ONE_BELOW);
-                        oy = fminf(fmaxf((float)(yc - (double)iy), 0.f), ONE_BELOW);
-                        vx = (float)(a.d_vx[pid] * k.inv_v64);
-                        vy = (float)(a.d_vy[pid] * k.inv_v64);
-                        qm = (float)a.d_qm[pid];
-                        spc = a.d_spc[pid];
-                        steps = a.d_steps[pid];
-                        stop_at = min(a.max_steps, steps + a.step_budget);
+                        s.ix = min(max((int)xc, 0), C.nx - 1);
+                        s.iy = min((int)floor(yc), C.ny - 1);  // a start above the grid escapes at once
+                        s.ox = fminf(fmaxf((float)(xc - (double)s.ix), 0.f), ONE_BELOW);
+                        s.oy = fminf(fmaxf((float)(yc - (double)s.iy), 0.f), ONE_BELOW);
+                        s.vx = (float)(a.d_vx[pid] * k.inv_v64);
+                        s.vy = (float)(a.d_vy[pid] * k.inv_v64);
+                        s.qm = (float)a.d_qm[pid];
+                        s.spc = a.d_spc[pid];
+                        s.steps = a.d_steps[pid];
+                        s.stop_at = min(a.max_steps, s.steps + a.step_budget);
                     }
                 }
             }
         }
-        if (pid < 0) continue;
+        if (s.pid < 0) continue;
+        step_particle<SMEM>(k, C, s, t);
+    }
 
-        // ---- vacuum-weighted bilinear field (trench_charging_2d.py:492-509) ----
-        // corners (i0, j0) = (ix - 1 + hx, iy - 1 + hy) .. (i0 + 1, j0 + 1); in the halo-padded
-        // field i0 + 1 = ix + hx needs no wrap and the clipped rows need one clamp
-        const int hx = ox >= 0.5f ? 1 : 0, hy = oy >= 0.5f ? 1 : 0;
-        const float tx = hx ? ox - 0.5f : ox + 0.5f;
-        const float ty = hy ? oy - 0.5f : oy + 0.5f;
-        const int base = (ix + hx) * P + max(iy + hy, 0);
-        const tb_fcell c00 = F.at(base), c01 = F.at(base + 1);
-        const tb_fcell c10 = F.at(base + P), c11 = F.at(base + P + 1);
-        const float ux = 1.f - tx, uy = 1.f - ty;
-        const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
-        const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
-        const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
-        const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
-        const float qs = __fdividef(qm, fmaxf(sw, 1e-12f));
-        const float ax = qs * sex, ay = qs * sey;
-        // the start cell is the corner on the particle's side of each centre line; its
-        // interior flag says every 8-neighbour is vacuum, so a move of < 1 cell cannot
-        // touch a wall and the end-cell and corner checks are skipped
-        const float start_ey = hx ? (hy ? c00.ey : c01.ey) : (hy ? c10.ey : c11.ey);
-        const bool near = !(__float_as_uint(start_ey) & 1u);
-
-        // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
-        const float speed = sqrtf(vx * vx + vy * vy);
-        const float acc = sqrtf(ax * ax + ay * ay);
-        const float dt = __fdividef(cfl, speed + sqrtf(2.f * acc) + inv_v);
-        const float vxn = vx + ax * dt, vyn = vy + ay * dt;
-        const float sx = 0.5f * (vx + vxn) * dt, sy = 0.5f * (vy + vyn) * dt;
-        float nox = ox + sx, noy = oy + sy;
-        const bool gx = nox >= 1.f, lx = nox < 0.f, gy = noy >= 1.f, ly = noy < 0.f;
-        const int dix = gx ? 1 : (lx ? -1 : 0);
-        const int diy = gy ? 1 : (ly ? -1 : 0);
-        nox = fminf(gx ? nox - 1.f : (lx ? nox + 1.f : nox), ONE_BELOW);
-        noy = fminf(gy ? noy - 1.f : (ly ? noy + 1.f : noy), ONE_BELOW);
-        int nix = ix + dix;
-        nix = nix < 0 ? nx - 1 : (nix >= nx ? 0 : nix);
-        const int niy = iy + diy;
-        ++steps;
-        ++my_steps;
-        const bool escaped = niy >= ny;
-        bool hit_end = false, corner = false;
-        if (near && !escaped) {
-            hit_end = !F.vac((nix + 1) * P + max(niy, -1) + 1);
-            // both the column and the (clipped) row changed: a staircase corner may lie on
-            // the path between two vacuum cells (trench_charging_2d.py:614-621)
-            corner = tapered && !hit_end && dix != 0 && max(niy, 0) != max(iy, 0);
-        }
-
-        if (!(hit_end || corner || escaped || steps >= stop_at)) {
-            ix = nix; iy = niy; ox = nox; oy = noy; vx = vxn; vy = vyn;
-            continue;
-        }
-
-        // ---- rare path: wall contact, escape, or step cap ----
-        const int y0c = min(max(iy, 0), ny - 1);
-        const int iyn = min(max(niy, 0), ny - 1);
-        const int diy_e = iyn - y0c;     // rows clipped like the reference
-        bool hit = hit_end;
-        int dcell = nix * ny + iyn;
-        bool reflected = false;
-        if (hit ? first_face : corner) {
-            // first solid face crossed (trench_charging_2d.py:512-539) in cell units
-            const float inf = __int_as_float(0x7f800000);
-            const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - ox) / sx : inf;
-            const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - oy) / sy : inf;
-            const bool x_first = fx < fy;
-            const int ax_ = x_first ? nix : ix, ay_ = x_first ? y0c : y0c + diy_e;
-            const bool use_last = dix != 0 && diy_e != 0 && F.vac((ax_ + 1) * P + ay_ + 1);
-            const int cx = use_last ? nix : ax_, cy = use_last ? y0c + diy_e : ay_;
-            const bool face_x = use_last ? !x_first : x_first;
-            const int ccell = cx * ny + cy;
-            hit = !F.vac((cx + 1) * P + cy + 1);
-            dcell = ccell;
-            if (hit && barrier) {
-                const float4 b = __ldg(barrier_tab + ccell);
-                // neighbour the particle came from: W/E across an x face, S/N across a y face
-                const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
-                const float vn = face_x ? vxn : vyn;
-                if (0.5f * vn * vn < qm * dphi) {
-                    // reflect: the normal velocity flips, the position stays at the start point
-                    vx = face_x ? -vxn : vxn;
-                    vy = face_x ? vyn : -vyn;
-                    hit = false;
-                    reflected = true;
+    if (pool != nullptr) {
+        __shared__ int s_live;
+        const int T = blockDim.x;
+        if (threadIdx.x == 0) s_live = 0;
+        for (;;) {
+            __syncthreads();
+            if (s.pid >= 0) {
+                pool_put(pool, T, atomicAdd(&s_live, 1), s);
+                s.pid = -1;
+            }
+            __syncthreads();
+            const int live = s_live;
+            if (live == 0) break;
+            if ((int)threadIdx.x < live) pool_get(pool, T, threadIdx.x, s);
+            __syncthreads();
+            if (threadIdx.x == 0) s_live = 0;
+            if ((int)(threadIdx.x & ~31u) < live) {  // warp-uniform: this warp holds particles
+                for (int r = 0; r < TAIL_ROUND_STEPS; ++r) {
+                    if (__ballot_sync(FULL, s.pid >= 0) == 0u) break;
+                    if (s.pid >= 0) step_particle<SMEM>(k, C, s, t);
                 }
             }
-        }
-        if (!reflected) { ix = nix; iy = niy; ox = nox; oy = noy; vx = vxn; vy = vyn; }
-
-        int done = 0;
-        if (hit) {
-            if (dcell < 0 || dcell >= cells) {
-                atomicCAS(err, TB_DERR_NONE, TB_DERR_BAD_CELL);
-            } else {
-                atomicAdd(a.d_counts + (size_t)spc * cells + dcell, 1);
-            }
-            if (a.d_hit) a.d_hit[pid] = dcell;
-            if (spc == 0) ++my_hit_i; else ++my_hit_e;
-            done = 1;
-        } else if (escaped && !reflected) {
-            if (spc == 0) ++my_esc_i; else ++my_esc_e;
-            done = 2;
-        } else if (steps >= stop_at) {
-            if (steps >= a.max_steps) ++my_lost;
-            done = 3;
-        }
-        if (done) {
-            a.d_steps[pid] = steps;
-            if (done != 3) a.d_status[pid] = (int8_t)done;
-            if (done == 3 || a.write_state) {
-                a.d_x[pid] = ((double)ix + (double)ox) * k.dx;
-                a.d_y[pid] = ((double)iy + (double)oy) * k.dx;
-                a.d_vx[pid] = (double)vx * k.vscale;
-                a.d_vy[pid] = (double)vy * k.vscale;
-            }
-            pid = -1;
         }
     }
 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        my_steps += __shfl_down_sync(FULL, my_steps, o);
-        my_esc_i += __shfl_down_sync(FULL, my_esc_i, o);
-        my_esc_e += __shfl_down_sync(FULL, my_esc_e, o);
-        my_lost += __shfl_down_sync(FULL, my_lost, o);
-        my_hit_i += __shfl_down_sync(FULL, my_hit_i, o);
-        my_hit_e += __shfl_down_sync(FULL, my_hit_e, o);
+        t.steps += __shfl_down_sync(FULL, t.steps, o);
+        t.esc_i += __shfl_down_sync(FULL, t.esc_i, o);
+        t.esc_e += __shfl_down_sync(FULL, t.esc_e, o);
+        t.lost += __shfl_down_sync(FULL, t.lost, o);
+        t.hit_i += __shfl_down_sync(FULL, t.hit_i, o);
+        t.hit_e += __shfl_down_sync(FULL, t.hit_e, o);
     }
     if (lane == 0) {
-        unsigned long long *t = reinterpret_cast<unsigned long long *>(a.d_totals);
-        if (my_esc_i) atomicAdd(t + 0, (unsigned long long)my_esc_i);
-        if (my_esc_e) atomicAdd(t + 1, (unsigned long long)my_esc_e);
-        if (my_lost) atomicAdd(t + 2, (unsigned long long)my_lost);
-        if (my_steps) atomicAdd(t + 3, (unsigned long long)my_steps);
-        if (my_hit_i) atomicAdd(t + 4, (unsigned long long)my_hit_i);
-        if (my_hit_e) atomicAdd(t + 5, (unsigned long long)my_hit_e);
+        unsigned long long *tot = reinterpret_cast<unsigned long long *>(a.d_totals);
+        if (t.esc_i) atomicAdd(tot + 0, (unsigned long long)t.esc_i);
+        if (t.esc_e) atomicAdd(tot + 1, (unsigned long long)t.esc_e);
+        if (t.lost) atomicAdd(tot + 2, (unsigned long long)t.lost);
+        if (t.steps) atomicAdd(tot + 3, (unsigned long long)t.steps);
+        if (t.hit_i) atomicAdd(tot + 4, (unsigned long long)t.hit_i);
+        if (t.hit_e) atomicAdd(tot + 5, (unsigned long long)t.hit_e);
     }
 }
 
@@ -320,7 +420,8 @@ __global__ void __launch_bounds__(THREADS, 1) trace_f32_kernel(const __grid_cons
         }
         fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
     }
-    run_case<SMEM>(k, fieldp);
+    uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
+    run_case<SMEM>(k, fieldp, pool);
 }
 
 // Many cases in one persistent launch: each CTA repeatedly takes the case with the
@@ -366,7 +467,8 @@ __global__ void __launch_bounds__(F32_THREADS, 1)
             staged = true;
             fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
         }
-        run_case<SMEM>(k, fieldp);
+        uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
+        run_case<SMEM>(k, fieldp, pool);
         __syncthreads();  // every warp is done with this case's field
     }
 }
@@ -444,8 +546,12 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.queue = ctx->d_queue;
     k.err = ctx->d_err;
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
+    k.pool_off = -1;
     return k;
 }
+
+// Bytes of the drain pool for a block of `threads`.
+int pool_bytes(int threads) { return POOL_WORDS * 4 * threads; }
 
 }  // namespace
 
@@ -466,20 +572,28 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
-    // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning); several
-    // CTAs per SM only when their shared-memory fields fit side by side
+    // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
     const int threads = ctx->tune_threads;
+    // the drain pool goes after the field when both fit (without the field it always fits
+    // under the default 48 KB)
+    const int pb = pool_bytes(threads);
+    size_t shm = smem ? (size_t)k.bytes : 0;
+    k.pool_off = -1;
+    if (ctx->nx < 65536 && ctx->ny < 32767 && (!smem || k.bytes + pb <= ctx->smem_attr_bytes)) {
+        k.pool_off = (int)shm;
+        shm += pb;
+    }
+    // several CTAs per SM only when their shared memory fits side by side
     int per_sm = ctx->tune_ctas_per_sm;
-    if (smem && (long long)per_sm * (k.bytes + 1024) > ctx->smem_per_sm) per_sm = 1;
+    if ((long long)per_sm * ((long long)shm + 1024) > ctx->smem_per_sm) per_sm = 1;
     long long want = (a->n + threads - 1) / threads;
     long long cap = (long long)ctx->num_sms * per_sm;
     int blocks = (int)(want < cap ? want : cap);
     if (blocks < 1) blocks = 1;
-    const size_t shm = smem ? (size_t)k.bytes : 0;
 #define TB_LAUNCH_F32(T)                                                                        \
     do {                                                                                        \
         if (smem) trace_f32_kernel<true, T><<<blocks, T, shm, s>>>(k);                         \
-        else trace_f32_kernel<false, T><<<blocks, T, 0, s>>>(k);                               \
+        else trace_f32_kernel<false, T><<<blocks, T, shm, s>>>(k);                             \
     } while (0)
     if (threads == 512) TB_LAUNCH_F32(512);
     else if (threads == 768) TB_LAUNCH_F32(768);
@@ -600,6 +714,8 @@ struct tb_pack {
     int max_bytes = 0;
     int max_particles = 0;
     bool smem = false;
+    int pool_off = -1;   // drain pool offset in dynamic shared memory, -1 = none
+    size_t shm = 0;      // dynamic shared memory of the launch
     int num_sms = 0;
     int ready = 0;
     char err[512] = {0};
@@ -644,6 +760,13 @@ extern "C" int tb_pack_create(tb_pack **out, int n_cases, tb_ctx *const *ctxs) {
     for (int i = 0; i < n_cases; ++i)
         p->max_bytes = std::max(p->max_bytes, tb_halo_count(ctxs[i]->nx, ctxs[i]->ny) * (int)sizeof(tb_fcell));
     p->smem = p->max_bytes <= ctxs[0]->smem_attr_bytes;
+    p->shm = p->smem ? (size_t)p->max_bytes : 0;
+    bool small_sides = true;
+    for (int i = 0; i < n_cases; ++i) small_sides = small_sides && ctxs[i]->nx < 65536 && ctxs[i]->ny < 32767;
+    if (small_sides && (!p->smem || p->max_bytes + pool_bytes(F32_THREADS) <= ctxs[0]->smem_attr_bytes)) {
+        p->pool_off = (int)p->shm;
+        p->shm += pool_bytes(F32_THREADS);
+    }
     cudaError_t e = cudaSetDevice(dev);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_cases, sizeof(K32) * n_cases);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_queues, sizeof(unsigned long long) * n_cases);
@@ -690,6 +813,7 @@ extern "C" int tb_pack_set_args(tb_pack *p, const tb_trace_args *args) {
         ks[i] = make_k32(p->ctxs[i], &a);
         ks[i].queue = p->d_queues + i;
         ks[i].err = p->d_err;
+        ks[i].pool_off = p->pool_off;
         p->max_particles = std::max<int>(p->max_particles, (int)a.n);
     }
     cudaError_t e = cudaSetDevice(p->device);
@@ -711,9 +835,9 @@ extern "C" int tb_pack_trace(tb_pack *p, int reset, void *stream) {
         k_pack_reset<<<dim3(blocks, p->n), 256, 0, s>>>(p->d_cases, p->n);
     }
     if (p->smem)
-        trace_f32_batch_kernel<true><<<p->num_sms, F32_THREADS, p->max_bytes, s>>>(p->d_cases, p->n, p->d_err);
+        trace_f32_batch_kernel<true><<<p->num_sms, F32_THREADS, p->shm, s>>>(p->d_cases, p->n, p->d_err);
     else
-        trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, 0, s>>>(p->d_cases, p->n, p->d_err);
+        trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, p->shm, s>>>(p->d_cases, p->n, p->d_err);
     e = cudaGetLastError();
     if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
     return TB_OK;

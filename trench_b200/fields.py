@@ -158,11 +158,17 @@ class FieldSolver:
     """
 
     RTOL = 1e-13
+    # The FP64 residual b - L x of an n-cell grid cannot be computed below a roundoff floor
+    # that grows with the grid (measured: 1.8e-13 relative at 560,000 cells, where 1e-13 is
+    # out of reach); the target is RTOL, or 5e-16 sqrt(n) on grids above 40,000 cells.
+    # A relative residual of 4e-13 moves the potential by about 1e-7 V.
+    RTOL_PER_SQRT_CELL = 5e-16
 
     def __init__(self, ctx, p, eps, cond, driven, max_rhs=64):
         self.ctx = ctx
         self.nx, self.ny = eps.shape
         self.n = self.nx * self.ny
+        self.rtol = max(self.RTOL, self.RTOL_PER_SQRT_CELL * float(np.sqrt(self.n)))
         self.dev = torch.device("cuda", ctx.device)
         self.dx2 = p.dx ** 2
         self.diag, self.ce, self.cn = poisson_matrix_arrays(eps, cond, p)
@@ -211,7 +217,7 @@ class FieldSolver:
             b = bp[s:e].contiguous()
             x = out[s:e].contiguous()
             self.ctx.check(L.tb_poisson_solve(self.ctx.handle, e - s, ctypes.c_void_p(b.data_ptr()),
-                                              ctypes.c_void_p(x.data_ptr()), self.RTOL, 40, self.inner,
+                                              ctypes.c_void_p(x.data_ptr()), self.rtol, 40, self.inner,
                                               ctypes.byref(iters), ctypes.byref(resid),
                                               ctypes.c_void_p(stream.cuda_stream)))
             out[s:e] = x
