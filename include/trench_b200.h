@@ -101,6 +101,12 @@ int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream
  * and 1 or 2 CTAs per SM (2 only where two shared-memory fields fit on an SM).
  * Chosen by the autotuner (ChargingCase.autotune); default 1024 x 1. */
 int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
+/* Order in which the FP32 tracer's lanes claim particles: 0 in index order
+ * (default), 1 from the last index down.  Results do not depend on it; the time
+ * does, because the launch ends with the longest trajectories claimed last (in a
+ * batch of ions then electrons whose electrons run longest, reverse order drains
+ * sooner).  Chosen by the autotuner. */
+int tb_set_claim_order(tb_ctx *ctx, int reverse);
 
 /* Synchronise `stream`, then read and clear the context's device-side check flag:
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the

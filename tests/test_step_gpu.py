@@ -301,14 +301,20 @@ def test_autotuners_pick_a_shape_and_keep_results(case_cls):
     parts = inject.inject(p, p.n_per_batch, tuned.ny, np.random.default_rng(3))
     tuned.load(*parts)
     timings = tuned.autotune_tracer()
-    assert set(timings) == set(tuned.TRACER_SHAPES)
-    counts = []
+    assert set(timings) == {(t, c, o) for t, c in tuned.TRACER_SHAPES for o in (0, 1)}
+    counts, hits = [], []
     from trench_b200 import _capi
-    for shape in tuned.TRACER_SHAPES:
-        assert _capi.lib().tb_set_tuning(tuned.ctx.handle, *shape) == 0
+    tuned.hit = torch.full((tuned.capacity,), -1, dtype=torch.int32, device=tuned.dev)
+    for t, c, o in sorted(timings):
+        assert _capi.lib().tb_set_tuning(tuned.ctx.handle, t, c) == 0
+        assert _capi.lib().tb_set_claim_order(tuned.ctx.handle, o) == 0
         tuned._trace_only(2 * p.n_per_batch)
         torch.cuda.synchronize()
         counts.append(tuned.counts.cpu().numpy().copy())
-    for c in counts[1:]:
+        hits.append(torch.where(tuned.status[:2 * p.n_per_batch] == 1, tuned.hit[:2 * p.n_per_batch], -1).cpu().numpy())
+    for c, h in zip(counts[1:], hits[1:]):
         np.testing.assert_array_equal(c, counts[0])
+        np.testing.assert_array_equal(h, hits[0])
     assert "poisson_schedule" in tuned.tuning and "tracer_shape" in tuned.tuning
+    assert tuned.tuning["claim_order"] in ("index", "reverse")
+    assert _capi.lib().tb_set_claim_order(tuned.ctx.handle, 2) == _capi.TB_ERR_ARG

@@ -130,6 +130,7 @@ SIGNATURES = {
     "tb_trace": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs), ctypes.c_int, _vp]),
     "tb_check": (ctypes.c_int, [_vp, _vp]),
     "tb_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "tb_set_claim_order": (ctypes.c_int, [_vp, ctypes.c_int]),
     "tb_poisson_setup": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int]),
     "tb_poisson_levels": (ctypes.c_int, [_vp]),
     "tb_poisson_schedule": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

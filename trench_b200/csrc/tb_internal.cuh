@@ -90,6 +90,7 @@ struct tb_ctx {
     int smem_per_sm = 0;                 // shared memory of one SM (bytes)
     int tune_threads = 1024;             // FP32 tracer CTA size (tb_set_tuning)
     int tune_ctas_per_sm = 1;            // FP32 tracer CTAs per SM
+    int tune_reverse = 0;                // FP32 tracer claims particles from the last index down
     tb_poisson *poisson = nullptr;        // multigrid hierarchy (tb_poisson_setup)
     char err[512] = {0};
 };

@@ -43,6 +43,7 @@ struct K32 {
     int *err;
     int bytes;                      // packed field bytes (multiple of 16)
     int pool_off;                   // byte offset of the drain pool in dynamic shared memory, -1 = none
+    int reverse;                    // claim particles from the last index down
 };
 
 // 1.0f for a vacuum cell, 0.0f for a solid one, with integer operations only
@@ -254,7 +255,10 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
 // (struct of arrays over the block's threads): pid; ix | iy << 16 (grids below 32768
 // cells a side, iy >= -1); steps; stop_at | spc << 31; ox, oy, vx, vy, qm.
 constexpr int POOL_WORDS = 9;
-constexpr int TAIL_ROUND_STEPS = 32;
+#ifndef TB_TAIL_ROUND_STEPS
+#define TB_TAIL_ROUND_STEPS 64
+#endif
+constexpr int TAIL_ROUND_STEPS = TB_TAIL_ROUND_STEPS;
 
 __device__ __forceinline__ void pool_put(uint32_t *P, int T, int q, const LaneState &s) {
     P[0 * T + q] = (uint32_t)s.pid;
@@ -338,7 +342,10 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                 base = __shfl_sync(FULL, base, leader);
                 if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
                 if (s.pid < 0) {
-                    const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
+                    // claim order: index order, or from the last index down (k.reverse)
+                    const unsigned long long rank = base + __popc(need & ((1u << lane) - 1u));
+                    const unsigned long long idx =
+                        (k.reverse && rank < (unsigned long long)a.n) ? (unsigned long long)a.n - 1 - rank : rank;
                     if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
                         const int pid = (int)idx;
                         s.pid = pid;
@@ -547,6 +554,7 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.err = ctx->d_err;
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     k.pool_off = -1;
+    k.reverse = ctx->tune_reverse;
     return k;
 }
 
@@ -570,6 +578,7 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.queue = ctx->d_queue;
     k.err = ctx->d_err;
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
+    k.reverse = ctx->tune_reverse;
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
@@ -858,6 +867,13 @@ extern "C" int tb_pack_check(tb_pack *p, void *stream) {
     return TB_OK;
 }
 
+
+extern "C" int tb_set_claim_order(tb_ctx *ctx, int reverse) {
+    if (!ctx) return TB_ERR_ARG;
+    if (reverse != 0 && reverse != 1) return tb_fail(ctx, TB_ERR_ARG, "tb_set_claim_order: order must be 0 or 1");
+    ctx->tune_reverse = reverse;
+    return TB_OK;
+}
 
 extern "C" int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm) {
     if (!ctx) return TB_ERR_ARG;

@@ -357,31 +357,35 @@ class ChargingCase:
     TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2))
 
     def autotune_tracer(self, n=None, reps=2):
-        """Times the tracer's launch shapes (CTA size, CTAs per SM) on the loaded batch and
-        keeps the fastest.  Traces only: neither the charge state nor the loaded batch is
-        changed (the trace is deterministic, so every shape gives the same counts)."""
+        """Times the tracer's launch shapes (CTA size, CTAs per SM) and claim orders (index
+        order or from the last index down) on the loaded batch and keeps the fastest.
+        Traces only: neither the charge state nor the loaded batch is changed (the trace
+        is deterministic, so every setting gives the same counts)."""
         L = _capi.lib()
         n = self.n_loaded if n is None else n
-        p = self.p
         timings = {}
         saved = self.trace_events
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         self.trace_events = (e0, e1)
         try:
-            for threads, per_sm in self.TRACER_SHAPES:
-                self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
-                best = float("inf")
-                for _ in range(reps):
-                    self._trace_only(n)
-                    e1.synchronize()
-                    best = min(best, e0.elapsed_time(e1))
-                timings[(threads, per_sm)] = best
+            for order in (0, 1):
+                self.ctx.check(L.tb_set_claim_order(self.ctx.handle, order))
+                for threads, per_sm in self.TRACER_SHAPES:
+                    self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
+                    best = float("inf")
+                    for _ in range(reps):
+                        self._trace_only(n)
+                        e1.synchronize()
+                        best = min(best, e0.elapsed_time(e1))
+                    timings[(threads, per_sm, order)] = best
         finally:
             self.trace_events = saved
-        shape = min(timings, key=timings.get)
-        self.ctx.check(L.tb_set_tuning(self.ctx.handle, *shape))
-        self.tuning["tracer"] = {f"{t}x{c}": v for (t, c), v in timings.items()}
-        self.tuning["tracer_shape"] = shape
+        threads, per_sm, order = min(timings, key=timings.get)
+        self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
+        self.ctx.check(L.tb_set_claim_order(self.ctx.handle, order))
+        self.tuning["tracer"] = {f"{t}x{c}{'-reverse' if o else ''}": v for (t, c, o), v in timings.items()}
+        self.tuning["tracer_shape"] = (threads, per_sm)
+        self.tuning["claim_order"] = "reverse" if order else "index"
         return timings
 
     def _trace_only(self, n):
