@@ -175,8 +175,19 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     if (near && !escaped) {
         hit_end = !C.F.vac((nix + 1) * P + max(niy, -1) + 1);
         // both the column and the (clipped) row changed: a staircase corner may lie on
-        // the path between two vacuum cells (trench_charging_2d.py:614-621)
+        // the path between two vacuum cells (trench_charging_2d.py:614-621).  The move
+        // reaches the wall only if the cell beyond the first boundary crossed is solid
+        // (the first-face rule of the rare path below, same expressions), so that is
+        // decided here and the rare path runs only for an actual corner contact.
         corner = C.tapered && !hit_end && dix != 0 && max(niy, 0) != max(s.iy, 0);
+        if (corner) {
+            const int y0c = min(max(s.iy, 0), ny - 1);
+            const int iyn = min(max(niy, 0), ny - 1);
+            const float fx = ((dix > 0 ? 1.f : 0.f) - s.ox) / sx;
+            const float fy = ((iyn > y0c ? 1.f : 0.f) - s.oy) / sy;
+            const bool x_first = fx < fy;
+            corner = !C.F.vac((x_first ? nix + 1 : s.ix + 1) * P + (x_first ? y0c : iyn) + 1);
+        }
     }
 
     if (!(hit_end || corner || escaped || s.steps >= s.stop_at)) {
