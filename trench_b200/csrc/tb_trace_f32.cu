@@ -159,17 +159,17 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     const float dt = __fdividef(C.cfl, speed + sqrtf(2.f * acc) + C.inv_v);
     const float vxn = s.vx + ax * dt, vyn = s.vy + ay * dt;
     const float sx = 0.5f * (s.vx + vxn) * dt, sy = 0.5f * (s.vy + vyn) * dt;
-    float nox = s.ox + sx, noy = s.oy + sy;
-    const bool gx = nox >= 1.f, lx = nox < 0.f, gy = noy >= 1.f, ly = noy < 0.f;
-    const int dix = gx ? 1 : (lx ? -1 : 0);
-    const int diy = gy ? 1 : (ly ? -1 : 0);
-    nox = fminf(gx ? nox - 1.f : (lx ? nox + 1.f : nox), ONE_BELOW);
-    noy = fminf(gy ? noy - 1.f : (ly ? noy + 1.f : noy), ONE_BELOW);
+    // a step moves less than one cell, so the new offset lies in (-1, 2): the cell
+    // change is its floor (-1, 0 or 1) and the new offset the remainder (exact for the
+    // shift by 1; a remainder that rounds up to 1 is clamped below 1)
+    const float fnx = floorf(s.ox + sx), fny = floorf(s.oy + sy);
+    const int dix = (int)fnx, diy = (int)fny;
+    const float nox = fminf((s.ox + sx) - fnx, ONE_BELOW);
+    const float noy = fminf((s.oy + sy) - fny, ONE_BELOW);
     int nix = s.ix + dix;
     nix = nix < 0 ? nx - 1 : (nix >= nx ? 0 : nix);
     const int niy = s.iy + diy;
     ++s.steps;
-    ++t.steps;
     const bool escaped = niy >= ny;
     bool hit_end = false, corner = false;
     if (near && !escaped) {
@@ -250,6 +250,7 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     }
     if (done) {
         const int pid = s.pid;
+        t.steps += (unsigned)s.steps;   // the claim subtracted the particle's earlier steps
         a.d_steps[pid] = s.steps;
         if (done != 3) a.d_status[pid] = (int8_t)done;
         if (done == 3 || a.write_state) {
@@ -373,6 +374,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                         s.spc = a.d_spc[pid];
                         s.steps = a.d_steps[pid];
                         s.stop_at = min(a.max_steps, s.steps + a.step_budget);
+                        t.steps -= (unsigned)s.steps;   // steps are tallied when the particle stops
                     }
                 }
             }
