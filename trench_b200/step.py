@@ -579,6 +579,7 @@ class HostPipeline:
         self.copy = torch.cuda.Stream(case.dev)
         self.copied = [torch.cuda.Event(), torch.cuda.Event()]
         self.done = [torch.cuda.Event(), torch.cuda.Event()]
+        self.row_dev = [torch.empty(case.hist_cols, dtype=torch.float64, device=case.dev) for _ in range(2)]
 
     def _stage(self, k, batch, after):
         X, SPC = self.case._inputs[k % 2]
@@ -602,9 +603,16 @@ class HostPipeline:
                 # buffer (k+1)%2 is free once batch k-1 has finished with it
                 self._stage(k + 1, batches[k + 1], self.done[(k + 1) % 2] if k >= 1 else start)
             self.graphs[k % 2].replay()
+            if rows is not None:
+                # the history row is gathered on the compute stream and read back on the copy
+                # stream, so the device-to-host transfer stays off the compute path
+                last = self.case.batch.clamp(0, self.case.max_batches - 1).long()
+                self.row_dev[k % 2].copy_(self.case.hist.index_select(0, last).squeeze(0))
             self.done[k % 2].record(comp)
             if rows is not None:
-                last = self.case.batch.clamp(0, self.case.max_batches - 1).long()
-                rows[k].copy_(self.case.hist.index_select(0, last).squeeze(0), non_blocking=True)
+                self.copy.wait_event(self.done[k % 2])
+                with torch.cuda.stream(self.copy):
+                    rows[k].copy_(self.row_dev[k % 2], non_blocking=True)
             if between is not None:
                 between()
+        comp.wait_stream(self.copy)   # the last history rows are on the host when the stream is done
