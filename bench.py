@@ -80,7 +80,7 @@ class Clocks:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -482,6 +482,7 @@ def run_large(args):
     clocks.start()
     before = case.batches_done()
     ms, trace_ms = [], []
+    torch.cuda.nvtx.range_push("timed")
     for _ in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -491,6 +492,7 @@ def run_large(args):
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
         trace_ms.append(t0e.elapsed_time(t1e))
+    torch.cuda.nvtx.range_pop()
     clk = clocks.stop()
     case.check()
     h = case.history()
