@@ -109,6 +109,14 @@ struct LaneState {
     float ox, oy, vx, vy, qm;
 };
 
+// The four bilinear corners a lane loaded last and their base index (-1 = none).  With
+// the field in global memory a step that stays in the same cell quad reuses them: a
+// move is under half a cell at the usual CFL, so about half the steps skip the gathers.
+struct QuadCache {
+    int base;
+    tb_fcell c00, c01, c10, c11;
+};
+
 // Per-lane event counts, reduced over the warp at the end.
 struct LaneTally {
     unsigned steps, esc_i, esc_e, lost, hit_i, hit_e;
@@ -128,7 +136,8 @@ struct CaseView {
 // wall entry and barrier reflection; on absorption, escape or the step cap the
 // particle's outputs are written and s.pid becomes -1.
 template <bool SMEM>
-__device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM> &C, LaneState &s, LaneTally &t) {
+__device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM> &C, LaneState &s, LaneTally &t,
+                                              QuadCache &q) {
     const tb_trace_args &a = k.a;
     const int nx = C.nx, ny = C.ny, P = C.P;
     // ---- vacuum-weighted bilinear field (trench_charging_2d.py:492-509) ----
@@ -138,8 +147,18 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     const float tx = hx ? s.ox - 0.5f : s.ox + 0.5f;
     const float ty = hy ? s.oy - 0.5f : s.oy + 0.5f;
     const int base = (s.ix + hx) * P + max(s.iy + hy, 0);
-    const tb_fcell c00 = C.F.at(base), c01 = C.F.at(base + 1);
-    const tb_fcell c10 = C.F.at(base + P), c11 = C.F.at(base + P + 1);
+    tb_fcell c00, c01, c10, c11;
+    if (SMEM) {
+        c00 = C.F.at(base); c01 = C.F.at(base + 1);
+        c10 = C.F.at(base + P); c11 = C.F.at(base + P + 1);
+    } else {
+        if (base != q.base) {
+            q.c00 = C.F.at(base); q.c01 = C.F.at(base + 1);
+            q.c10 = C.F.at(base + P); q.c11 = C.F.at(base + P + 1);
+            q.base = base;
+        }
+        c00 = q.c00; c01 = q.c01; c10 = q.c10; c11 = q.c11;
+    }
     const float ux = 1.f - tx, uy = 1.f - ty;
     const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
     const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
@@ -337,6 +356,9 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     s.ix = s.iy = s.steps = s.stop_at = s.spc = 0;
     s.ox = s.oy = s.vx = s.vy = s.qm = 0.f;
     LaneTally t = {0u, 0u, 0u, 0u, 0u, 0u};
+    QuadCache q;
+    q.base = -1;
+    q.c00 = q.c01 = q.c10 = q.c11 = tb_fcell{0.f, 0.f};
     bool open = true;
 
     for (;;) {
@@ -361,6 +383,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                     if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
                         const int pid = (int)idx;
                         s.pid = pid;
+                        q.base = -1;
                         // metres -> cells: x lies in cell min(int(x/dx), nx-1) as in the
                         // reference (trench_charging_2d.py:611)
                         const double xc = a.d_x[pid] * k.inv_dx, yc = a.d_y[pid] * k.inv_dx;
@@ -380,7 +403,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
             }
         }
         if (s.pid < 0) continue;
-        step_particle<SMEM>(k, C, s, t);
+        step_particle<SMEM>(k, C, s, t, q);
     }
 
     if (pool != nullptr) {
@@ -397,12 +420,13 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
             const int live = s_live;
             if (live == 0) break;
             if ((int)threadIdx.x < live) pool_get(pool, T, threadIdx.x, s);
+            q.base = -1;
             __syncthreads();
             if (threadIdx.x == 0) s_live = 0;
             if ((int)(threadIdx.x & ~31u) < live) {  // warp-uniform: this warp holds particles
                 for (int r = 0; r < TAIL_ROUND_STEPS; ++r) {
                     if (__ballot_sync(FULL, s.pid >= 0) == 0u) break;
-                    if (s.pid >= 0) step_particle<SMEM>(k, C, s, t);
+                    if (s.pid >= 0) step_particle<SMEM>(k, C, s, t, q);
                 }
             }
         }
