@@ -113,6 +113,16 @@ int tb_configure_trace_f32(tb_ctx *ctx);
 int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
                           const double *wface, double vscale, cudaStream_t s);
 
+// Deposits one particle into counts[key] (key = species * cells + cell).  Warp-aggregated:
+// the lanes of the warp that deposit into the same key at this point add once, with
+// the number of such lanes.  The counts are integers, so the result is exact and
+// independent of the order of the additions.
+__device__ __forceinline__ void tb_deposit(int32_t *counts, size_t key) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, (unsigned long long)key);
+    if ((int)(threadIdx.x & 31u) == __ffs(peers) - 1) atomicAdd(counts + key, __popc(peers));
+}
+
 // Periodic index helpers.
 __host__ __device__ __forceinline__ int tb_wrap(int i, int n) {
     return i < 0 ? i + n : (i >= n ? i - n : i);

@@ -255,7 +255,7 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         if (dcell < 0 || dcell >= C.cells) {
             atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BAD_CELL);
         } else {
-            atomicAdd(a.d_counts + (size_t)s.spc * C.cells + dcell, 1);
+            tb_deposit(a.d_counts, (size_t)s.spc * C.cells + dcell);
         }
         if (a.d_hit) a.d_hit[s.pid] = dcell;
         if (s.spc == 0) ++t.hit_i; else ++t.hit_e;

@@ -269,7 +269,7 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
             if (cell < 0 || cell >= cells) {
                 atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BAD_CELL);
             } else {
-                atomicAdd(a.d_counts + (size_t)spc * cells + cell, 1);
+                tb_deposit(a.d_counts, (size_t)spc * cells + cell);
             }
             if (a.d_hit) a.d_hit[pid] = (int32_t)cell;
             if (spc == 0) ++my_hit_i; else ++my_hit_e;
