@@ -12,8 +12,9 @@
 //
 // The charge update over those deposits is the recurrence of tb_step_charge
 // (trench_charging_2d.py:1239-1266: deposit, leakage, driven or floating
-// conductor), same arithmetic in the same order, so at r = 1 it reproduces the
-// traced run's surface charge.  Its adjoint, per batch in reverse, with
+// conductor), same arithmetic, so at r = 1 it reproduces the traced run's surface
+// charge (to the rounding of the real-valued sums, which tb_step_charge may add in
+// another order).  Its adjoint, per batch in reverse, with
 // lambda = dJ / d rho_{b+1}:
 //   floating conductor  rho_{b+1} = r' + e_c C (dV - drift) / dx^2,
 //                       drift = dx^2 sum_s g_s (r'_s - rho_b,s), dV = f(ni, ne, drift)

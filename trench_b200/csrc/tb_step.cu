@@ -17,9 +17,12 @@
 //
 // Compiled with -fmad=false so the field and deposit arithmetic rounds like
 // the reference's NumPy expressions.
+#include <cooperative_groups.h>
 #include <math.h>
 
 #include "tb_internal.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -155,6 +158,116 @@ __global__ void __launch_bounds__(ONE_BLOCK) k_finish(const tb_step_desc d, cons
     }
 }
 
+// Fused charge update (K1 + leakage GEMV + K3 in one launch) for m <= FUSED_MAX_M
+// surface slots: one cluster of FUSED_CTAS blocks.  Each block takes a contiguous range
+// of slots for the per-slot work and every warp of the cluster a share of the leakage
+// rows; the phases are separated by cluster barriers (release/acquire at cluster scope,
+// which orders the global-memory writes of one phase before the reads of the next).
+// Per-block partial sums are combined by block 0 through distributed shared memory in
+// rank order, so the result does not depend on scheduling.
+constexpr int FUSED_CTAS = 8;
+constexpr int FUSED_MAX_M = 1024;
+
+__global__ void __cluster_dims__(FUSED_CTAS, 1, 1) __launch_bounds__(ONE_BLOCK)
+    k_charge_fused(const tb_step_desc d, int ncell, int *err) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    __shared__ double sh[32];
+    __shared__ double part[10];  // ni, ne, bi, be, hi, he, reg | reg_new, drift
+    const double dx2 = d.dx * d.dx;
+    const int m = d.m;
+    const int per = (m + FUSED_CTAS - 1) / FUSED_CTAS;
+    const int s0 = rank * per, s1 = min(m, s0 + per);
+    // ---- deposit and leakage input (k_deposit) ----
+    double ni = 0, ne = 0, bi = 0, be = 0, hi = 0, he = 0, reg = 0;
+    for (int s = s0 + (int)threadIdx.x; s < s1; s += blockDim.x) {
+        const int c = d.d_surf[s];
+        const int ci = d.d_counts[c], ce = d.d_counts[ncell + c];
+        const uint8_t f = d.d_sflag[s];
+        const double rp = d.d_rho_s[s];
+        d.d_rho_prev[s] = rp;
+        double drho = ((double)(ci - ce) * d.q_macro) / dx2;
+        if (f & TB_SFLAG_COND) drho = 0.0;
+        const double r = rp + drho;
+        d.d_rho_s[s] = r;
+        const double qs = r * dx2;
+        d.d_work[s] = d.d_leak_h ? qs + d.d_leak_h[s] : qs;
+        if (f & TB_SFLAG_COND) { ni += ci; ne += ce; }
+        if (f & TB_SFLAG_BOTTOM) { bi += ci; be += ce; }
+        if (f & TB_SFLAG_REGION) reg += qs;
+        hi += ci;
+        he += ce;
+    }
+    ni = block_reduce(ni, sh); ne = block_reduce(ne, sh);
+    bi = block_reduce(bi, sh); be = block_reduce(be, sh);
+    hi = block_reduce(hi, sh); he = block_reduce(he, sh);
+    reg = block_reduce(reg, sh);
+    if (threadIdx.x == 0) {
+        part[0] = ni; part[1] = ne; part[2] = bi; part[3] = be; part[4] = hi; part[5] = he; part[6] = reg;
+    }
+    cl.sync();
+    // ---- leakage: work[m + r] = M[r] . work[0, m), one warp per row over the cluster ----
+    const bool leak = d.d_leak_M != nullptr;
+    if (leak) {
+        const int wpb = blockDim.x >> 5, lane = threadIdx.x & 31;
+        for (int r = rank * wpb + (int)(threadIdx.x >> 5); r < m; r += FUSED_CTAS * wpb) {
+            const double *row = d.d_leak_M + (size_t)r * m;
+            double acc = 0.0;
+            for (int c = lane; c < m; c += 32) acc += row[c] * d.d_work[c];
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+            if (lane == 0) d.d_work[m + r] = acc;
+        }
+    }
+    cl.sync();
+    // ---- leakage result, driven conductor, drift (k_finish, per slot) ----
+    double reg_new = 0, drift = 0;
+    for (int s = s0 + (int)threadIdx.x; s < s1; s += blockDim.x) {
+        const uint8_t f = d.d_sflag[s];
+        double r = d.d_rho_s[s];
+        if (leak) {
+            const double qn = d.d_work[m + s];
+            r = qn / dx2;
+            if (f & TB_SFLAG_REGION) reg_new += qn;
+        }
+        if (d.driven && (f & TB_SFLAG_COND)) r = 0.0;
+        d.d_rho_s[s] = r;
+        if (d.floating) drift += (r - d.d_rho_prev[s]) * d.d_g_s[s];
+    }
+    reg_new = block_reduce(reg_new, sh);
+    drift = block_reduce(drift, sh);
+    if (threadIdx.x == 0) { part[7] = reg_new; part[8] = drift; }
+    cl.sync();
+    // ---- conductor step and history (k_finish, block 0 thread 0) ----
+    if (rank == 0 && threadIdx.x == 0) {
+        double t[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int b = 0; b < FUSED_CTAS; ++b) {
+            const double *pb = cl.map_shared_rank(part, b);
+            for (int i = 0; i < 9; ++i) t[i] += pb[i];
+        }
+        // every absorbed particle must have landed on a surface cell
+        if ((long long)t[4] != d.d_totals[4] || (long long)t[5] != d.d_totals[5])
+            atomicCAS(err, TB_DERR_NONE, TB_DERR_OFF_SURFACE);
+        const int row = ++*d.d_batch;
+        double leak_ratio = 0.0;
+        if (leak) leak_ratio = (t[6] - t[7]) / d.dt_batch / d.leak_norm;
+        if (d.floating && d.c_slot >= 0) {
+            const double dr = t[8] * dx2;
+            const double dV = conductor_step(t[0], t[1], d.q_macro, d.C_cond, d.Te, dr);
+            d.d_rho_s[d.c_slot] += d.C_cond * (dV - dr) / dx2;
+        }
+        if (row >= 0 && row < d.max_batches) {
+            double *h = d.d_hist + (size_t)row * d.hist_cols;
+            h[H_RATIO_I] = t[2] / d.bottom_norm;
+            h[H_RATIO_E] = t[3] / d.bottom_norm;
+            h[H_ESC_E] = (double)d.d_totals[1] / d.n_per_batch;
+            h[H_LOST] = (double)d.d_totals[2] / (2.0 * d.n_per_batch);
+            h[H_LEAK] = leak_ratio;
+            h[H_STEPS] = (double)d.d_totals[3];
+        }
+    }
+    cl.sync();  // block 0 has read every block's partial sums before any block exits
+}
+
 // K5: E = -grad phi over vacuum neighbours (trench_charging_2d.py:429-454), the
 // packed FP32 tracer field, the per-face wall barrier and the probe history.
 __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac, double scale_e, double scale_phi,
@@ -221,6 +334,12 @@ extern "C" int tb_step_charge(tb_ctx *ctx, const tb_step_desc *d, void *stream) 
         return tb_fail(ctx, TB_ERR_ARG, "tb_step_charge: leakage needs dt_batch and leak_norm");
     TB_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = (cudaStream_t)stream;
+    if (d->m <= FUSED_MAX_M) {
+        k_charge_fused<<<FUSED_CTAS, ONE_BLOCK, 0, s>>>(*d, ctx->nx * ctx->ny, ctx->d_err);
+        TB_CUDA(ctx, cudaGetLastError());
+        return TB_OK;
+    }
+    // many surface slots: the leakage GEMV runs over the whole GPU between two one-block kernels
     double *tally = reinterpret_cast<double *>(ctx->d_queue + 2);  // 5 doubles of context scratch
     k_deposit<<<1, ONE_BLOCK, 0, s>>>(*d, ctx->nx * ctx->ny, tally, ctx->d_err);
     if (d->d_leak_M) {
