@@ -134,6 +134,15 @@ def measured_peaks():
         return {}
 
 
+def profile_issue():
+    """Warp instructions per particle-step of the FP32 tracer from the committed ncu summary."""
+    try:
+        d = json.loads((ROOT / "profiles" / "trace_f32_issue.json").read_text())
+        return float(d["warp_instructions_per_particle_step"]), int(d["sms"]), int(d["schedulers_per_sm"])
+    except Exception:
+        return None
+
+
 def profile_traffic():
     """DRAM bytes per particle of the FP32 tracer from the committed ncu summary, if any."""
     try:
@@ -339,6 +348,16 @@ def run_b200(args, p):
             "kernel": "trace_f32_kernel", "trace_ms_per_launch": float(np.mean(trace_ms)),
             "particle_steps_per_launch": mean_steps,
             "particle_steps_per_s": float(np.mean([s / (t / 1000.0) for s, t in zip(steps_per_batch, trace_ms)]))}
+    issue = profile_issue()
+    if issue and clk and clk.get("sm_mhz"):
+        # the binding limit of this kernel: one warp instruction per scheduler per cycle
+        per_step, sms, sched = issue
+        ach = per_step * float(np.mean([s / (t / 1000.0) for s, t in zip(steps_per_batch, trace_ms)]))
+        peak = sms * sched * clk["sm_mhz"] * 1e6
+        roof["issue"] = {"achieved": ach, "peak": peak, "unit": "warp instructions/s", "frac": ach / peak,
+                         "warp_instructions_per_particle_step": per_step,
+                         "source": "profiles/trace_f32_issue.json (ncu) x live particle-steps/s; peak = "
+                                   "SMs x 4 schedulers x sampled SM clock"}
     cpu = cpu_baseline(p, 1 << 15, seconds_budget=args.cpu_seconds)
     line = {"metric": METRIC, "value": value, "unit": "particles/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
