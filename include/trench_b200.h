@@ -183,6 +183,12 @@ int tb_step_charge(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
 /* Potential on the needed cells, FP64 field, packed FP32 tracer field (as
  * tb_set_fields) and probe history. */
 int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
+/* Charge monitors of the history (trench_charging_2d.py:871-874, 1281-1285): for each
+ * of n_monitors, dx^2 sum_s weights[r][s] rho_s (or |rho_s| where absolute[r] != 0)
+ * over the m surface slots, written to row *d_batch of d_out (max_batches, n_monitors).
+ * Call after tb_step_charge. */
+int tb_step_monitors(tb_ctx *ctx, const tb_step_desc *desc, const double *d_weights, const uint8_t *d_absolute,
+                     int n_monitors, double *d_out, void *stream);
 
 /* ---- Device-side injection -------------------------------------------------------
  * Samples n_species ions (indices [0, n)) then n_species electrons ([n, 2n)) into the

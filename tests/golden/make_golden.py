@@ -14,6 +14,10 @@ Fixtures:
                 (trench_charging_2d.py:1045-1369)
   fields_*.npz  setup_fields / solve / compute_field / build_leakage /
                 conductor_response outputs for one geometry
+  steady_checks.npz  the steady-state check functions on seeded synthetic histories
+                (trench_charging_2d.py:877-945)
+  steady_run_*.npz  run() with until_steady to convergence: histories, charge
+                monitors, convergence batch
   regression_pin.json  agreement of run() here with the reference's own
                 tests/data/*.npz (tests/test_regression.py:41-50)
 """
@@ -272,6 +276,54 @@ def main(ref):
         T.inject = orig_inject
     save("run_cfg1_30.npz", params=params_json(cfg1_run), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
          solid=res["solid"], mask=res["mask"], **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
+
+    # --- steady-state stopping (until_steady) -----------------------------------
+    # the check functions on seeded synthetic histories (trench_charging_2d.py:877-945)
+    rs = np.random.default_rng(77)
+    series = []
+    for k in range(12):
+        n = 30
+        t = np.arange(n)
+        x = rs.normal(0, 1 + k % 3, n) + (0.05 * k) * t
+        if k % 4 == 3:
+            x = np.cumsum(x) * 0.1   # strongly autocorrelated
+        series.append(x)
+    series = np.array(series)
+    mse = np.array([T._mean_and_se(x) for x in series])
+    sp = replace(P(), steady_window=15, steady_rtol=0.005, steady_charge_rtol=0.005, steady_charge_atol=1e-15,
+                 dt_batch=1e-4)
+    probe_names = ["a", "b", "c"]
+    vcases, ccases = [], []
+    for k in range(6):
+        h = {nm: list(20 + rs.normal(0, 0.05, 30) + (0.02 * k * (j + 1)) * np.arange(30) / 30)
+             for j, nm in enumerate(probe_names)}
+        ok, name, d, tol = T.check_steady(h, probe_names, sp, None)
+        vcases.append(([h[nm] for nm in probe_names], [float(ok), probe_names.index(name), d, tol]))
+        q = {nm: list(1e-12 * (1 + rs.normal(0, 0.01, 30) + 0.01 * k * np.arange(30) / 30))
+             for nm in ("left", "right")}
+        c = T.check_charge_steady(q, sp)
+        ccases.append(([q["left"], q["right"]],
+                       [float(c["ok"]), ["left", "right"].index(c["name"]), float(c["kind"] == "drift"),
+                        c["d"], c["tol"], c["ratio"], c["rate"]]))
+    save("steady_checks.npz", params=params_json(sp), series=series, mean_se=mse,
+         v_hist=np.array([v[0] for v in vcases]), v_out=np.array([v[1] for v in vcases]),
+         q_hist=np.array([c[0] for c in ccases]), q_out=np.array([c[1] for c in ccases]))
+    # whole runs to steady charge
+    steady_runs = {
+        "floating": replace(P(), sigma_s=1e-14, until_steady=True, max_batches=400, steady_window=5, steady_hold=2,
+                            **{k: v for k, v in base.items() if k != "n_batches"}),
+        "dielectric": replace(P(), sigma_s=1e-14, mask_type="dielectric", until_steady=True, max_batches=400,
+                              steady_window=10, steady_hold=2, **{k: v for k, v in base.items() if k != "n_batches"}),
+    }
+    for name, p in steady_runs.items():
+        res = T.run(p, log=lambda s: None)
+        save(f"steady_run_{name}.npz", params=params_json(p), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
+             converged=np.array(res["converged"]), t_conv=np.array(res["t_conv"]),
+             steady_n_ok=np.array(res["checkpoint"]["steady_n_ok"]),
+             steady_names=np.array(list(res["steady"])), steady_values=np.array(list(res["steady"].values())),
+             **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()},
+             **{f"charge_{k}": np.asarray(v) for k, v in res["charge_hist"].items()},
+             **{f"monitor_{k}": np.asarray(v) for k, v in res["charge_monitor_hist"].items()})
 
     # --- agreement with the reference's own regression data -------------------
     pin = {}

@@ -191,6 +191,34 @@ def test_fp32_batch_loop_tracks_reference_cfg1_full_run(case_cls):
     assert np.max(np.abs(res["mean_phi"] - g["mean_phi"])) <= 0.02 * swing
 
 
+@pytest.mark.parametrize("name", ["floating", "dielectric"])
+def test_until_steady_stops_where_the_reference_does(case_cls, name):
+    """run() with until_steady (FP64 tracer): the steady-state check passes at the same
+    batch as the reference run(), with the
+    same potential and charge-monitor histories and the same steady values."""
+    g = load_golden(f"steady_run_{name}.npz")
+    p = g["p"]
+    case = case_cls(p, precision="f64", green="f64")
+    res = case.run()
+    assert res["converged"] == bool(g["converged"])
+    assert res["t_conv"] == pytest.approx(float(g["t_conv"]), rel=1e-12)
+    assert len(res["hist"]["t"]) == len(g["hist_t"])
+    for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
+        np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])
+    for k in case.probes:
+        np.testing.assert_allclose(res["hist"][k], g[f"hist_{k}"], rtol=1e-10, atol=1e-8)
+    for k, v in res["charge_monitor_hist"].items():
+        want = g[f"monitor_{k}"]
+        np.testing.assert_allclose(v, want, rtol=1e-9, atol=1e-9 * max(np.abs(want).max(), 1e-30))
+    for k in ("left", "right"):
+        np.testing.assert_allclose(res["charge_hist"][k], g[f"charge_{k}"], rtol=1e-9, atol=1e-25)
+    want = dict(zip([str(n) for n in g["steady_names"]], g["steady_values"]))
+    for k, v in res["steady"].items():
+        assert v == pytest.approx(want[k], rel=1e-10, abs=1e-8)
+    assert res["checkpoint"]["steady_n_ok"] == int(g["steady_n_ok"])
+    np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-13 * np.abs(g["rho_raw"]).max())
+
+
 def test_graph_replay_equals_eager(case_cls):
     """A captured batch replays the same kernels: same counts as an eager batch."""
     import torch

@@ -138,6 +138,7 @@ SIGNATURES = {
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(_dbl), _vp]),
     "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
+    "tb_step_monitors": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp, _vp, ctypes.c_int, _vp, _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
     "tb_inject": (ctypes.c_int, [_vp, ctypes.POINTER(InjectArgs), _vp]),
     "tb_philox_fill": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int, _vp, _vp]),

@@ -268,6 +268,27 @@ __global__ void __cluster_dims__(FUSED_CTAS, 1, 1) __launch_bounds__(ONE_BLOCK)
     cl.sync();  // block 0 has read every block's partial sums before any block exits
 }
 
+// Charge monitors of the history (trench_charging_2d.py:871-874, 1281-1285): for each
+// monitor r, dx^2 sum_s w[r][s] x (|rho_s| if absolute[r] else rho_s) into row
+// *d_batch of out.  Charge only sits on surface slots, so the monitors' cell sets are
+// weights over the slots; one warp per monitor.
+__global__ void k_monitors(const tb_step_desc d, const double *w, const uint8_t *absolute, int n, double *out) {
+    const int row = *d.d_batch;
+    if (row < 0 || row >= d.max_batches) return;
+    const int lane = threadIdx.x & 31;
+    for (int r = threadIdx.x >> 5; r < n; r += blockDim.x >> 5) {
+        const double *wr = w + (size_t)r * d.m;
+        const bool ab = absolute[r] != 0;
+        double acc = 0.0;
+        for (int s = lane; s < d.m; s += 32) {
+            const double v = d.d_rho_s[s];
+            acc += wr[s] * (ab ? fabs(v) : v);
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[(size_t)row * n + r] = acc * (d.dx * d.dx);
+    }
+}
+
 // K5: E = -grad phi over vacuum neighbours (trench_charging_2d.py:429-454), the
 // packed FP32 tracer field, the per-face wall barrier and the probe history.
 __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac, double scale_e, double scale_phi,
@@ -376,3 +397,17 @@ extern "C" int tb_step_potential(tb_ctx *ctx, const tb_step_desc *d, void *strea
     ctx->fields_ready = 1;
     return TB_OK;
 }
+
+extern "C" int tb_step_monitors(tb_ctx *ctx, const tb_step_desc *d, const double *d_weights,
+                                const uint8_t *d_absolute, int n_monitors, double *d_out, void *stream) {
+    if (!ctx || !d) return TB_ERR_ARG;
+    if (n_monitors < 0 || (n_monitors > 0 && (!d_weights || !d_absolute || !d_out)) || d->m < 1 || !d->d_rho_s ||
+        !d->d_batch || !(d->dx > 0))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_step_monitors: invalid arguments");
+    if (n_monitors == 0) return TB_OK;
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    k_monitors<<<1, 256, 0, (cudaStream_t)stream>>>(*d, d_weights, d_absolute, n_monitors, d_out);
+    TB_CUDA(ctx, cudaGetLastError());
+    return TB_OK;
+}
+

@@ -20,7 +20,7 @@ from dataclasses import asdict, is_dataclass
 import numpy as np
 import torch
 
-from . import _capi, geometry
+from . import _capi, geometry, steady
 from .fields import FieldSolver, apply_matrix, boundary_rhs, compute_field, field_voltages
 from .inject import inject, launch_times
 from .params import E_CHARGE, EPS0, WALL_MODELS, is_tapered
@@ -129,7 +129,7 @@ class ChargingCase:
             sflag[(sy == p.floor_t - 1) & (sx >= b0) & (sx < b1)] |= _capi.SFLAG_BOTTOM
             self.q_macro = E_CHARGE * (p.flux * (nx * p.dx) * p.dt_batch / p.n_per_batch)
             # device state
-            self.max_batches = int(max_batches or max(p.n_batches, 1))
+            self.max_batches = int(max_batches or (p.max_batches if p.until_steady else max(p.n_batches, 1)))
             self.hist_cols = len(HIST_SCALARS) + len(self.probes)
             cap = int(capacity or 2 * p.n_per_batch)
             self.capacity = cap
@@ -149,6 +149,21 @@ class ChargingCase:
             self.t_probes = torch.from_numpy(probe_flat.astype(np.int32)).to(dev)
             self.batch = torch.full((1,), -1, dtype=torch.int32, device=dev)
             self.counts = torch.zeros((2, self.n), dtype=torch.int32, device=dev)
+            # charge monitors (trench_charging_2d.py:850-874): weights over the surface slots
+            regions = steady.charge_monitors(solid, mask, i0, i1, p)
+            self.monitor_names = list(regions) + ["surface absolute"]
+            slot = -np.ones(self.n, dtype=np.int64)
+            slot[S] = np.arange(m)
+            mw = np.zeros((len(self.monitor_names), m))
+            for r, cells in enumerate(regions.values()):
+                js = slot[cells]
+                mw[r, js[js >= 0]] = 1.0
+            mw[-1] = mw[list(regions).index("surface")]
+            absolute = np.zeros(len(self.monitor_names), np.uint8)
+            absolute[-1] = 1
+            self.t_mon_w = torch.from_numpy(mw).to(dev)
+            self.t_mon_abs = torch.from_numpy(absolute).to(dev)
+            self.qhist = torch.zeros((self.max_batches, len(self.monitor_names)), dtype=f64, device=dev)
             self.totals = torch.zeros(8, dtype=torch.int64, device=dev)
             self.X = [torch.zeros(cap, dtype=f64, device=dev) for _ in range(5)]  # x, y, vx, vy, qm
             self.SPC = torch.zeros(cap, dtype=torch.int8, device=dev)
@@ -353,6 +368,8 @@ class ChargingCase:
             self.after_trace()
         self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
         self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
+        self.ctx.check(L.tb_step_monitors(self.ctx.handle, ctypes.byref(self._desc), _ptr(self.t_mon_w),
+                                          _ptr(self.t_mon_abs), len(self.monitor_names), _ptr(self.qhist), s))
 
     TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2))
 
@@ -447,6 +464,13 @@ class ChargingCase:
         out["t"] = np.arange(1, nb + 1) * self.p.dt_batch
         return out
 
+    def charge_history(self):
+        """Charge monitors per batch (C/m): the reference's charge_monitor_hist; its
+        charge_hist is the 'left' and 'right' entries."""
+        nb = min(self.batches_done(), self.max_batches)
+        q = self.qhist[:nb].cpu().numpy()
+        return {k: q[:, r].copy() for r, k in enumerate(self.monitor_names)}
+
     def rho(self):
         r = np.zeros(self.n)
         r[self.S] = self.rho_s.cpu().numpy()
@@ -468,10 +492,12 @@ class ChargingCase:
         self.check()
         params = asdict(self.p) if is_dataclass(self.p) else dict(vars(self.p))
         return dict(rho_raw=self.rho(), hist=self.history(), params=params,
+                    charge_monitor_hist=self.charge_history(),
                     checkpoint=dict(version=CHECKPOINT_VERSION, batches_completed=self.batches_done(),
                                     rng_state=rng.bit_generator.state if rng is not None else None,
                                     phase_rng_state=phase_rng.bit_generator.state if phase_rng is not None
-                                    else None))
+                                    else None,
+                                    steady_n_ok=int(getattr(self, "_steady_n_ok", 0))))
 
     def restore(self, res):
         """Continue from a checkpoint of this backend or a reference result of the same case
@@ -495,11 +521,20 @@ class ChargingCase:
         for j, k in enumerate(self.probes):
             if k in hist:
                 rows[:, len(HIST_SCALARS) + j] = np.asarray(hist[k], dtype=np.float64)[:done]
+        # charge monitors: the saved ones, NaN where the result has none (the steady-state
+        # check then starts after them, as the reference's steady_history_start does)
+        mon = res.get("charge_monitor_hist", {}) or {}
+        qrows = np.full((done, len(self.monitor_names)), np.nan)
+        for r, k in enumerate(self.monitor_names):
+            if k in mon and len(mon[k]) >= done:
+                qrows[:, r] = np.asarray(mon[k], dtype=np.float64)[:done]
         with torch.cuda.device(self.dev):
             self.rho_s.copy_(torch.from_numpy(rho.ravel()[self.S].copy()))
             self.hist.zero_()
+            self.qhist.zero_()
             if done:
                 self.hist[:done].copy_(torch.from_numpy(rows))
+                self.qhist[:done].copy_(torch.from_numpy(qrows))
             self.batch.fill_(done - 1)
             self._potential()
             torch.cuda.current_stream(self.dev).synchronize()
@@ -509,6 +544,8 @@ class ChargingCase:
         ck = self.checkpoint(rng, phase_rng)
         np.savez(path, rho_raw=ck["rho_raw"], params_json=json.dumps(ck["params"]),
                  checkpoint_json=json.dumps(ck["checkpoint"]),
+                 monitor_names_json=json.dumps(list(ck["charge_monitor_hist"])),
+                 monitors=np.array(list(ck["charge_monitor_hist"].values())),
                  **{f"hist_{k}": v for k, v in ck["hist"].items()})
 
     @staticmethod
@@ -518,6 +555,8 @@ class ChargingCase:
             res = dict(rho_raw=d["rho_raw"], params=json.loads(str(d["params_json"])),
                        checkpoint=json.loads(str(d["checkpoint_json"])),
                        hist={k[5:]: d[k] for k in d.files if k.startswith("hist_")})
+            if "monitor_names_json" in d.files:
+                res["charge_monitor_hist"] = dict(zip(json.loads(str(d["monitor_names_json"])), d["monitors"]))
         return res
 
     @staticmethod
@@ -527,12 +566,20 @@ class ChargingCase:
         rng.bit_generator.state = state
         return rng
 
-    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None, resume=None):
-        """The reference batch loop (trench_charging_2d.py:1225-1285) with host injection;
-        `resume` (a checkpoint or loaded file) continues a saved run for n_batches more."""
+    STEADY_SETTINGS = ("until_steady", "steady_window", "steady_rtol", "steady_charge_rtol",
+                       "steady_charge_atol", "steady_hold")
+
+    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None, resume=None, stop=None):
+        """The reference batch loop (trench_charging_2d.py:1199-1369) with host injection.
+        Without until_steady it runs n_batches (default p.n_batches) more batches; with
+        until_steady it runs until the steady-state check (potential probes and charge
+        monitors, every steady_window batches) has passed steady_hold times in a row or
+        p.max_batches batches are done.  `resume` (a checkpoint or loaded file, or a
+        reference result) continues a saved run; `stop` (an object with is_set()) ends
+        the loop between batches."""
         p = self.p
-        n_batches = p.n_batches if n_batches is None else n_batches
         phase_rng = None
+        n_ok = 0
         if resume is not None:
             self.restore(resume)
             ck = resume.get("checkpoint") or {}
@@ -540,6 +587,10 @@ class ChargingCase:
                 rng = self.restore_rng(ck["rng_state"])
             if self.rf is not None and ck.get("phase_rng_state"):
                 phase_rng = self.restore_rng(ck["phase_rng_state"])
+            src = resume.get("params") or {}
+            if p.until_steady and ck.get("steady_n_ok") is not None and all(
+                    src.get(k) == getattr(p, k) for k in self.STEADY_SETTINGS):
+                n_ok = int(ck["steady_n_ok"])
         rng = np.random.default_rng(p.seed) if rng is None else rng
         if p.field_mode in ("circuit", "circuit_rf") and ion_energy is None and ion_velocity is None:
             # ions start at the plasma potential with the Bohm energy (trench_charging_2d.py:1135-1139)
@@ -547,8 +598,29 @@ class ChargingCase:
         if phase_rng is None and self.rf is not None:
             phase_rng = np.random.default_rng(np.random.SeedSequence([p.seed, 0x5246]))
         self._rngs = (rng, phase_rng)
+        start = self.batches_done()
+        if p.until_steady:
+            n_max = int(p.max_batches)
+        else:
+            n_max = start + int(p.n_batches if n_batches is None else n_batches)
+        if n_max > self.max_batches:
+            raise ValueError(f"{n_max} batches exceed this case's history of {self.max_batches} "
+                             "(ChargingCase(max_batches=...))")
+        W = int(p.steady_window)
+        probes = list(self.probes)
+        # potentials are compared with the external ones only under the RF circuit
+        # (trench_charging_2d.py:1167-1168)
+        reference = ({k: float(self.external[ix, iy]) for k, (ix, iy) in self.probes.items()}
+                     if self.rf is not None else None)
+        first = 0
+        if p.until_steady and start:
+            first = steady.history_start(self.history(), probes, self.charge_history())
+        converged_at, stopped, check = None, False, None
         with torch.cuda.device(self.dev):
-            for b in range(n_batches):
+            for b in range(start, n_max):
+                if stop is not None and stop.is_set():
+                    stopped = True
+                    break
                 parts = inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity)
                 t0 = None
                 if phase_rng is not None:
@@ -557,11 +629,38 @@ class ChargingCase:
                 self.load(*parts, launch_times=t0)
                 self.step()
                 if log is not None and ((b + 1) % 10 == 0 or b == 0):
-                    log(f"[{b + 1}/{n_batches}]")
+                    log(f"[{b + 1}/{n_max}]")
+                if p.until_steady and (b + 1) % W == 0 and (b + 1) - first >= 2 * W:
+                    hist, mon = self.history(), self.charge_history()
+                    v_ok, name, d, tol = steady.check_steady(hist, probes, p, reference)
+                    charge = steady.check_charge_steady(mon, p)
+                    ok = bool(v_ok and charge["ok"])
+                    n_ok = min(n_ok + 1, p.steady_hold) if ok else 0
+                    check = dict(ok=ok, n_ok=n_ok, voltage=dict(ok=bool(v_ok), name=name, d=float(d), tol=float(tol)),
+                                 charge=charge)
+                    if log is not None:
+                        log(f"  steady check: potential {'OK' if v_ok else 'NG'} ({name} {d:+.3g} V, tol {tol:.3g}), "
+                            f"charge {'OK' if charge['ok'] else 'NG'} ({charge['name']} {charge['kind']}) "
+                            f"-> {n_ok}/{p.steady_hold}")
+                    if n_ok >= p.steady_hold:
+                        converged_at = b + 1
+                        break
             self.check()
+        self._steady_n_ok = n_ok
         ex, ey = self.fields()
+        hist = self.history()
         ck = self.checkpoint(rng, phase_rng)["checkpoint"]
-        return dict(rho_raw=self.rho(), mean_phi=self.full_potential(), Ex=ex, Ey=ey, hist=self.history(),
+        mon = self.charge_history()
+        Wl = min(W, len(hist["t"]))
+        steady_values = {k: float(hist[k][-Wl:].mean()) for k in probes} if Wl else {}
+        t_conv = converged_at * p.dt_batch if converged_at else np.nan
+        if p.until_steady and log is not None and not converged_at and not stopped:
+            log(f"not steady after {n_max} batches (raise max_batches)")
+        params = asdict(p) if is_dataclass(p) else dict(vars(p))
+        return dict(rho_raw=self.rho(), mean_phi=self.full_potential(), Ex=ex, Ey=ey, hist=hist,
+                    charge_hist={k: mon[k] for k in ("left", "right")}, charge_monitor_hist=mon,
+                    steady=steady_values, t_conv=t_conv, converged=converged_at is not None, stopped=stopped,
+                    check=check, start_batch=start, params=params,
                     solid=self.solid, mask=self.mask, probes=self.probes, backend_used="b200", checkpoint=ck)
 
 
