@@ -328,6 +328,7 @@ def run_b200(args, p):
             dist.destroy_process_group()
         return 0
     adj = adjoint_measure() if (args.adjoint and world == 1) else None
+    to_steady = steady_measure(p) if (args.steady and world == 1) else None
 
     particles = n * args.steps * world
     value = particles / (total_ms / 1000.0)
@@ -374,6 +375,7 @@ def run_b200(args, p):
                     "batches_per_s": 1000.0 * args.steps * world / e2e_total},
             "device_injection": dinj,
             "adjoint": adj,
+            "to_steady": to_steady,
             "gpu_launches": 10 * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "wall_s": wall}
@@ -603,6 +605,35 @@ def device_injection(case, p, steps):
                     "history row read back each step"}
 
 
+def steady_measure(p):
+    """The AR-8 workload run to steady charge (configuration 2: until_steady, at most
+    3000 batches, the reference's default window 30 and hold 2), each batch drawn on the
+    device and replayed from a CUDA graph; the steady-state check reads the history back
+    every window."""
+    import time
+    import torch
+    from trench_b200 import inject
+    from trench_b200.step import ChargingCase
+    q = replace(p, until_steady=True, max_batches=3000, seed=p.seed + 7)
+    case = ChargingCase(q, precision="f32", green="f64")
+    et = inject.table_from_pdf(inject.bimodal_gaussian_pdf(40.0, 6.0, 140.0, 6.0), 0.0, 200.0)
+    at = inject.table_from_pdf(inject.half_gaussian_pdf(np.radians(3.0)), 0.0, np.radians(18.0))
+    inj = inject.DeviceInjector(case, seed=31, energy_table=et, angle_table=at)
+    inj(batch=10 ** 6)
+    case.autotune_tracer(2 * q.n_per_batch, reps=2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = case.run(injector=inj)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    nb = len(res["hist"]["t"])
+    return {"workload": "AR-8 RF-charging trench, 2^20 particles per batch drawn on the device, until_steady "
+                        "(window 30, hold 2, at most 3000 batches)",
+            "converged": bool(res["converged"]), "batches": nb, "seconds": wall, "batches_per_s": nb / wall,
+            "particles_per_s": nb * 2 * q.n_per_batch / wall,
+            "steady_potentials_V": {k: round(v, 3) for k, v in res["steady"].items()}}
+
+
 def adjoint_measure():
     """The adjoint on the AR-5 sensitivity workload (2^20 ions + 2^20 electrons per batch,
     50 batches, 64-bin IED, 32-bin IAD): recording time of the forward run (with 32
@@ -683,6 +714,8 @@ def main():
     ap.add_argument("--cases", type=int, default=64, help="cases of the sweep workload")
     ap.add_argument("--tracer-shape", default="auto",
                     help="auto (autotuned) or <threads>x<CTAs per SM>[-reverse], e.g. 1024x1-reverse")
+    ap.add_argument("--no-steady", dest="steady", action="store_false",
+                    help="skip the run to steady charge (AR-8 workload, 1 GPU only)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",
                     help="skip the adjoint measurement (AR-5 sensitivity workload, 1 GPU only)")
     args = ap.parse_args()

@@ -219,6 +219,29 @@ def test_until_steady_stops_where_the_reference_does(case_cls, name):
     np.testing.assert_allclose(res["rho_raw"], g["rho_raw"], rtol=1e-10, atol=1e-13 * np.abs(g["rho_raw"]).max())
 
 
+def test_device_injected_run_replays_like_eager_batches(case_cls):
+    """run(injector=...) (inject + step replayed from one CUDA graph) equals the same
+    batches injected and stepped one by one."""
+    import torch
+    from trench_b200 import inject as inj_mod
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc",
+                sigma_s=1e-14, n_per_batch=3000, n_batches=6)
+    et = inj_mod.table_from_pdf(inj_mod.bimodal_gaussian_pdf(40.0, 6.0, 140.0, 6.0), 0.0, 200.0, bins=64)
+    a, b = case_cls(p), case_cls(p)
+    ia = inj_mod.DeviceInjector(a, seed=5, energy_table=et)
+    ib = inj_mod.DeviceInjector(b, seed=5, energy_table=et)
+    res = a.run(injector=ia)
+    for _ in range(p.n_batches):
+        ib()
+        b.step()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(res["rho_raw"], b.rho())
+    hb = b.history()
+    for k in res["hist"]:
+        np.testing.assert_array_equal(res["hist"][k], hb[k])
+    np.testing.assert_array_equal(res["charge_monitor_hist"]["left"], b.charge_history()["left"])
+
+
 def test_graph_replay_equals_eager(case_cls):
     """A captured batch replays the same kernels: same counts as an eager batch."""
     import torch

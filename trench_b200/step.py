@@ -569,8 +569,11 @@ class ChargingCase:
     STEADY_SETTINGS = ("until_steady", "steady_window", "steady_rtol", "steady_charge_rtol",
                        "steady_charge_atol", "steady_hold")
 
-    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None, resume=None, stop=None):
-        """The reference batch loop (trench_charging_2d.py:1199-1369) with host injection.
+    def run(self, n_batches=None, rng=None, ion_energy=None, ion_velocity=None, log=None, resume=None, stop=None,
+            injector=None):
+        """The reference batch loop (trench_charging_2d.py:1199-1369) with host injection,
+        or with `injector` (an inject.DeviceInjector of this case) drawing every batch on
+        the device, each batch then replayed from one CUDA graph (inject + step).
         Without until_steady it runs n_batches (default p.n_batches) more batches; with
         until_steady it runs until the steady-state check (potential probes and charge
         monitors, every steady_window batches) has passed steady_hold times in a row or
@@ -616,18 +619,38 @@ class ChargingCase:
         if p.until_steady and start:
             first = steady.history_start(self.history(), probes, self.charge_history())
         converged_at, stopped, check = None, False, None
+        if injector is not None and self.rf is not None:
+            raise ValueError("device injection draws no RF launch phases; circuit_rf runs inject on the host")
+        graph = None
         with torch.cuda.device(self.dev):
             for b in range(start, n_max):
                 if stop is not None and stop.is_set():
                     stopped = True
                     break
-                parts = inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity)
-                t0 = None
-                if phase_rng is not None:
-                    t0 = np.concatenate([launch_times(phase_rng, p.n_per_batch, self.rf["period"])
-                                         for _ in range(2)])
-                self.load(*parts, launch_times=t0)
-                self.step()
+                if injector is not None:
+                    if graph is None and b > start:
+                        # inject + step as one graph; the injector's Philox batch word follows the
+                        # case's device batch counter, so every replay draws a new batch
+                        side = torch.cuda.Stream(self.dev)
+                        side.wait_stream(torch.cuda.current_stream(self.dev))
+                        graph = torch.cuda.CUDAGraph()
+                        with torch.cuda.stream(side), torch.cuda.graph(graph, stream=side):
+                            injector()
+                            self.step(2 * p.n_per_batch)
+                        torch.cuda.current_stream(self.dev).wait_stream(side)
+                    if graph is not None:
+                        graph.replay()
+                    else:
+                        injector()
+                        self.step()
+                else:
+                    parts = inject(p, p.n_per_batch, self.ny, rng, ion_energy, ion_velocity)
+                    t0 = None
+                    if phase_rng is not None:
+                        t0 = np.concatenate([launch_times(phase_rng, p.n_per_batch, self.rf["period"])
+                                             for _ in range(2)])
+                    self.load(*parts, launch_times=t0)
+                    self.step()
                 if log is not None and ((b + 1) % 10 == 0 or b == 0):
                     log(f"[{b + 1}/{n_max}]")
                 if p.until_steady and (b + 1) % W == 0 and (b + 1) - first >= 2 * W:
@@ -645,6 +668,7 @@ class ChargingCase:
                     if n_ok >= p.steady_hold:
                         converged_at = b + 1
                         break
+            del graph
             self.check()
         self._steady_n_ok = n_ok
         ex, ey = self.fields()
