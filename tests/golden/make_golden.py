@@ -171,10 +171,13 @@ def main(ref):
                               trench_taper_deg=tr, mask_taper_deg=ma, bias="dc", sigma_s=1e-14, n_per_batch=256,
                               max_steps=800, n_batches=3),
     }
+    display = lambda res: dict(rho_display=res["rho"], phi_display=res["phi"], external_phi=res["external_phi"],
+                               Ex_display=res["Ex"], Ey_display=res["Ey"],
+                               volts=np.array([res["voltages"][k] for k in ("substrate", "mask", "top")]))
     for name, p in runs.items():
         res = T.run(p, log=lambda s: None)
         save(f"run_{name}.npz", params=params_json(p), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
-             solid=res["solid"], mask=res["mask"],
+             solid=res["solid"], mask=res["mask"], **display(res),
              **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
 
     # circuit_rf batch loop with the reference's test waveform (tests/test_taper.py:273-283)
@@ -196,7 +199,7 @@ def main(ref):
         T.PC.solve_circuit_cached, T.PC.summary = orig_solve, orig_summary
     save("run_rf_taper.npz", params=params_json(rfrun), rho_raw=res["rho_raw"], mean_phi=res["mean_phi"],
          solid=res["solid"], mask=res["mask"], circuit_t=circ["t"], circuit_uw=circ["uw"], circuit_um=circ["um"],
-         circuit_up=circ["up"], circuit_V1=circ["V1"],
+         circuit_up=circ["up"], circuit_V1=circ["V1"], **display(res),
          **{f"hist_{k}": np.asarray(v) for k, v in res["hist"].items()})
 
     # --- vertical-ion probe (trench_charging_2d.py:1373-1439) -------------------

@@ -126,6 +126,21 @@ def test_fp64_batch_loop_matches_reference_run(case_cls, name):
     np.testing.assert_allclose(res["hist"]["leak"], g["hist_leak"], rtol=1e-9, atol=1e-12)
     for k in case.probes:
         np.testing.assert_allclose(res["hist"][k], g[f"hist_{k}"], rtol=1e-10, atol=1e-8)
+    check_display(res, g)
+
+
+def check_display(res, g):
+    """The result's display outputs: potential, charge with the conductor's induced
+    surface charge (trench_charging_2d.py:833-843), external potential, field, voltages."""
+    np.testing.assert_allclose(res["phi"], g["phi_display"], rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(res["external_phi"], g["external_phi"], rtol=1e-10, atol=1e-8)
+    scale = np.abs(g["rho_display"]).max()
+    np.testing.assert_allclose(res["rho"], g["rho_display"], rtol=1e-8, atol=1e-9 * scale)
+    escale = max(np.abs(g["Ex_display"]).max(), np.abs(g["Ey_display"]).max())
+    np.testing.assert_allclose(res["Ex"], g["Ex_display"], rtol=1e-8, atol=1e-9 * escale)
+    np.testing.assert_allclose(res["Ey"], g["Ey_display"], rtol=1e-8, atol=1e-9 * escale)
+    np.testing.assert_allclose([res["voltages"][k] for k in ("substrate", "mask", "top")], g["volts"],
+                               rtol=1e-12, atol=1e-12)
 
 
 def test_fp32_batch_loop_tracks_oracle(case_cls):
@@ -279,6 +294,7 @@ def test_rf_batch_loop_matches_reference_run(case_cls):
     np.testing.assert_allclose(res["mean_phi"], g["mean_phi"], rtol=1e-10, atol=1e-8)
     for k in ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost"):
         np.testing.assert_array_equal(res["hist"][k], g[f"hist_{k}"])
+    check_display(res, g)
 
 
 @pytest.mark.parametrize("mode", ["floating", "fixed", "dielectric"])

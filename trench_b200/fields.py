@@ -321,6 +321,20 @@ def setup_fields(p, solid, mask, circuit=None, device=0, max_rhs=64):
     return fields
 
 
+def conductor_surface_charge(rho, phi, solver, cond, boundary_rhs=None):
+    """Charge density for display and saving (trench_charging_2d.py:833-843): rho with the
+    conductor cells replaced by the induced surface charge -eps0 (A phi - b) that makes
+    them equipotential (during the run a conductor's charge is only a total, kept on one
+    cell)."""
+    out = np.array(rho, dtype=np.float64, copy=True)
+    if np.any(cond):
+        induced = apply_matrix(solver.diag, solver.ce, solver.cn, phi)
+        if boundary_rhs is not None:
+            induced = induced - boundary_rhs
+        out[cond] = (-EPS0 * induced)[cond]
+    return out
+
+
 def rf_coefficients(rf, at):
     """Periodic linear interpolation of the voltage deltas (trench_rf.py:5-11)."""
     wave = rf["wave"]

@@ -21,7 +21,8 @@ import numpy as np
 import torch
 
 from . import _capi, geometry, steady
-from .fields import FieldSolver, apply_matrix, boundary_rhs, compute_field, field_voltages
+from .fields import (FieldSolver, apply_matrix, boundary_rhs, compute_field, conductor_surface_charge,
+                     field_snapshot, field_voltages)
 from .inject import inject, launch_times
 from .params import E_CHARGE, EPS0, WALL_MODELS, is_tapered
 from .tracer import DEFAULT_VSCALE, Context, _ptr
@@ -69,6 +70,7 @@ class ChargingCase:
                 phi_cond = np.zeros((nx, ny))
                 mask_rhs = np.zeros((nx, ny))
             rhs = boundary_rhs(p, eps, volts)
+            self.boundary_rhs = rhs
             self.external = (solver.solve((rhs + mask_rhs).ravel()) + phi_cond.ravel()).reshape(nx, ny)
             self.floating = bool(cond.any() and not driven)
             self.driven = driven
@@ -212,12 +214,13 @@ class ChargingCase:
         period = (t[1] - t[0]) * t.size
         wave = np.column_stack((circuit["uw"] - circuit["up"], circuit["um"] - circuit["up"]))
         mean = wave.mean(axis=0)
-        basis = []
+        basis, rhs_basis = [], []
         for vs, vm in ((1.0, 0.0), (0.0, 1.0)):
             brhs = boundary_rhs(p, eps, dict(substrate=vs, mask=vm, top=0.0), fixed_sides=False)
             bc = cond.astype(float) * vm
             b = brhs - apply_matrix(solver.diag, solver.ce, solver.cn, bc)
             basis.append((solver.solve(b.ravel()) + bc.ravel()).reshape(nx, ny))
+            rhs_basis.append(brhs)
         basis = np.array(basis)
         electric = [compute_field(v, vac, p, 0.0) for v in basis]
         dt_max = period / p.rf_time_steps
@@ -225,7 +228,8 @@ class ChargingCase:
             dt_max = min(dt_max, p.rf_rise / 8)
         w = wave - mean
         self.rf = dict(period=float(period), wave=w, phi=basis, Ex=np.array([e[0] for e in electric]),
-                       Ey=np.array([e[1] for e in electric]), dt_max=float(dt_max))
+                       Ey=np.array([e[1] for e in electric]), dt_max=float(dt_max),
+                       boundary_rhs=np.array(rhs_basis))
         f = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
         self.t_rf = dict(ex=f(self.rf["Ex"]), ey=f(self.rf["Ey"]), phi=f(basis), wave=f(w))
         bound = np.abs(w).max(axis=0)
@@ -672,6 +676,13 @@ class ChargingCase:
             self.check()
         self._steady_n_ok = n_ok
         ex, ey = self.fields()
+        mean_phi = self.full_potential()
+        rho_raw = self.rho()
+        # display phase of circuit_rf (trench_charging_2d.py:416-426, 1355-1359)
+        shown_phi, external, shown_rhs, volts = field_snapshot(
+            dict(rf=self.rf, external=self.external, boundary_rhs=self.boundary_rhs, volts=self.volts), mean_phi, p)
+        if self.rf is not None:
+            ex, ey = compute_field(shown_phi, self.vac, p, volts["top"])
         hist = self.history()
         ck = self.checkpoint(rng, phase_rng)["checkpoint"]
         mon = self.charge_history()
@@ -681,7 +692,9 @@ class ChargingCase:
         if p.until_steady and log is not None and not converged_at and not stopped:
             log(f"not steady after {n_max} batches (raise max_batches)")
         params = asdict(p) if is_dataclass(p) else dict(vars(p))
-        return dict(rho_raw=self.rho(), mean_phi=self.full_potential(), Ex=ex, Ey=ey, hist=hist,
+        return dict(phi=shown_phi, mean_phi=mean_phi,
+                    rho=conductor_surface_charge(rho_raw, shown_phi, self.solver, self.cond, shown_rhs),
+                    Ex=ex, Ey=ey, rho_raw=rho_raw, external_phi=external, voltages=volts, hist=hist,
                     charge_hist={k: mon[k] for k in ("left", "right")}, charge_monitor_hist=mon,
                     steady=steady_values, t_conv=t_conv, converged=converged_at is not None, stopped=stopped,
                     check=check, start_batch=start, params=params,
