@@ -95,8 +95,21 @@ class B200Tracer:
         self.precision = precision
         self.vscale = float(vscale)
         self.tdev = torch.device("cuda", self.device)
-        self.last = {}
+        self._last_dev = None     # device outputs of the last call, read back on first use of .last
+        self._last_host = {}
         self._ctx_dx = None
+
+    @property
+    def last(self):
+        """Per-particle outputs of the last call (status, absorbing cell, steps) and its
+        particle-step total; copied to the host when first asked for."""
+        if self._last_dev is not None:
+            d = self._last_dev
+            self._last_host = dict(particle_steps=d["particle_steps"], precision=d["precision"],
+                                   status=d["status"].cpu().numpy(), hit=d["hit"].cpu().numpy(),
+                                   steps=d["steps"].cpu().numpy())
+            self._last_dev = None
+        return self._last_host
 
     # -- helpers ---------------------------------------------------------------
     def _dev(self, a, dtype):
@@ -147,7 +160,9 @@ class B200Tracer:
         stream = torch.cuda.current_stream(dev)
         sp = ctypes.c_void_p(stream.cuda_stream)
 
-        X = [self._dev(v, f64).clone() for v in (x, y, vx, vy)]
+        # the tracer writes particle state back (record, step budget): a caller's tensor is copied
+        X = [self._dev(v, f64) for v in (x, y, vx, vy)]
+        X = [t.clone() if isinstance(v, torch.Tensor) else t for t, v in zip(X, (x, y, vx, vy))]
         QM = self._dev(qm, f64)
         SPC = torch.from_numpy(np.ascontiguousarray(spc_h, dtype=np.int8)).to(dev)
         EX, EY = self._dev(Ex, f64), self._dev(Ey, f64)
@@ -227,12 +242,11 @@ class B200Tracer:
 
         cnt = counts.to(torch.int64).cpu().numpy()
         tot = totals.cpu().numpy()
-        host_status = status.cpu().numpy()
         escaped = np.array([tot[0], tot[1]], dtype=np.int64)
-        lost = int(np.count_nonzero(host_status == 3))
-        self.last = dict(particle_steps=int(tot[3]), status=host_status, hit=hit.cpu().numpy(),
-                         steps=steps.cpu().numpy(), precision=precision)
+        lost = int((status == 3).sum().item())
+        self._last_dev = dict(particle_steps=int(tot[3]), status=status, hit=hit, steps=steps, precision=precision)
         if record is not None:
+            host_status = self.last["status"]
             host_hit = self.last["hit"]
             cells = np.full((n, 2), -1, dtype=int)
             ab = host_status == 1
