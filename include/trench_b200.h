@@ -50,7 +50,8 @@ typedef struct {
     int step_budget;                 /* steps this launch (<= max_steps); chunked runs */
     double cfl;
     int tapered;                     /* corner crossing + first-face deposit (trench_charging_2d.py:554) */
-    /* circuit_rf in-flight clock (F64 only); n_phase = 0 disables */
+    /* circuit_rf in-flight clock; n_phase = 0 disables.  Precision F32 reads the
+       basis fields packed by tb_set_rf_fields instead of these three. */
     const double *d_rf_ex, *d_rf_ey, *d_rf_phi; /* (2, nx, ny) */
     const double *d_wave;            /* (n_phase, 2) */
     int n_phase;
@@ -90,6 +91,15 @@ int tb_device_info(const tb_ctx *ctx, char *name, int name_len, int *num_sms);
  * these arrays to the GPU on every call; here they stay resident. */
 int tb_set_fields(tb_ctx *ctx, const double *d_ex, const double *d_ey, const double *d_phi,
                   const double *d_wface, double vscale, void *stream);
+
+/* Pack the circuit_rf unit-voltage basis fields ((2, nx, ny) Ex, Ey and potential:
+ * substrate then mask electrode) for precision F32 with the RF clock: the fields as
+ * one float4 per cell and the per-face barrier of each basis potential, in the units
+ * of the last tb_set_fields (call it again after a tb_set_fields with another
+ * vscale).  The basis is fixed for a case, so one call serves every batch.  Replaces
+ * the copies of rf_ex/rf_ey/rf_phi in CudaTracer.__call__ (trench_cuda.py:63-70). */
+int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, const double *d_rf_phi,
+                     const double *d_wface, void *stream);
 
 /* Trace particles until absorbed, escaped or max_steps; deposit hits into
  * d_counts with integer atomics.  Replaces the chunk loop, kernel launch and host

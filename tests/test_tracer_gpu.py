@@ -133,6 +133,48 @@ def test_f32_large_sample_agreement_and_bottom_flux(tracers):
     assert agree >= 0.999, f"hit agreement {agree:.5f}"
 
 
+def test_f32_rf_hits_agree_with_fp64_oracle(tracers):
+    """circuit_rf in FP32 (basis fields, mid-step waveform, in-flight clock and RF wall
+    barrier): per-particle absorbing cells agree with the FP64 oracle on the fixture."""
+    g = load_golden("trace_rf_taper.npz")
+    t = tracers(g["solid"], "f32")
+    got = t(*parts(g), g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g), rf=rf_of(g))
+    assert t.last["precision"] == "f32"
+    want = OT.trace_detail(*parts(g)[:5], g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g), rf=rf_of(g))
+    same = (t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])
+    print(f"FP32 RF vs FP64 oracle: {same.mean():.5f} of {len(same)}")
+    assert same.mean() >= 0.99, f"agreement {same.mean():.5f}"
+    assert got[0].sum() + got[1].sum() + got[2].sum() + got[3] == len(same)
+
+
+def test_f32_rf_large_sample_agreement_and_bottom_flux(tracers):
+    """2^15 particles/species with uniform launch phases on the RF fixture's geometry and
+    fields: FP32 hit cells agree with the FP64 oracle for >= 99.9% and the bottom ion
+    and electron fluxes are within 3 sigma; a run split into 256-step launches (the
+    clock carried through the state arrays) agrees with the single launch."""
+    g = load_golden("trace_rf_taper.npz")
+    p, solid = g["p"], g["solid"]
+    rng = np.random.default_rng(77)
+    n = 1 << 15
+    x, y, vx, vy, qm, spc = inject.inject(p, n, solid.shape[1], rng)
+    rf = dict(rf_of(g), initial_time=rng.uniform(0.0, float(g["rf_period"]), 2 * n))
+    want = OT.trace_detail(x, y, vx, vy, qm, g["Ex"], g["Ey"], ~solid, p, barrier(g), rf=rf)
+    t = tracers(solid, "f32")
+    got = t(x, y, vx, vy, qm, spc, g["Ex"], g["Ey"], ~solid, p, barrier(g), rf=rf)
+    same = (t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])
+    print(f"FP32 RF vs FP64 oracle: hit agreement {same.mean():.6f} over {len(same)} particles")
+    assert same.mean() >= 0.999, f"hit agreement {same.mean():.5f}"
+    ref = OT.counts_from_detail(want, spc, solid.shape)
+    b0, b1 = geometry.opening_span(solid, p.floor_t)
+    for k in (0, 1):
+        a, r = got[k][b0:b1, p.floor_t - 1].sum(), ref[k][b0:b1, p.floor_t - 1].sum()
+        assert abs(a - r) <= 3 * np.sqrt(max(r, 1)), (k, a, r)
+    single = (t.last["status"].copy(), t.last["hit"].copy())
+    t(x, y, vx, vy, qm, spc, g["Ex"], g["Ey"], ~solid, p, barrier(g), rf=rf, stop=threading.Event())
+    chunked = (t.last["status"] == single[0]) & (t.last["hit"] == single[1])
+    assert chunked.mean() >= 0.999, f"chunked agreement {chunked.mean():.5f}"
+
+
 def test_global_memory_path_on_a_large_grid(tracers):
     """A 200x700 grid (2.5 nm cells, AR-10 trench 40 x 400 cells, dielectric mask 80):
     the packed FP32 field (1.1 MB) exceeds shared memory, so the FP32 tracer reads it

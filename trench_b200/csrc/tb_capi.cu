@@ -32,6 +32,8 @@ static int release(tb_ctx *c) {
     cudaFree(c->d_vac);
     cudaFree(c->d_field);
     cudaFree(c->d_barrier);
+    cudaFree(c->d_rf_field);
+    cudaFree(c->d_rf_barrier);
     cudaFree(c->d_queue);
     cudaFree(c->d_err);
     tb_poisson_free(c->poisson);
@@ -110,6 +112,22 @@ extern "C" int tb_set_fields(tb_ctx *ctx, const double *d_ex, const double *d_ey
     return tb_launch_pack_fields(ctx, d_ex, d_ey, d_phi, d_wface, vscale, (cudaStream_t)stream);
 }
 
+extern "C" int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, const double *d_rf_phi,
+                                const double *d_wface, void *stream) {
+    if (!ctx) return TB_ERR_ARG;
+    if (!d_rf_ex || !d_rf_ey || !d_rf_phi)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_set_rf_fields: the basis fields and potentials are required");
+    if (!ctx->fields_ready) return tb_fail(ctx, TB_ERR_ARG, "tb_set_rf_fields: call tb_set_fields first");
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const size_t cells = (size_t)ctx->nx * ctx->ny;
+    if (!ctx->d_rf_field) {
+        // allocated on first use: cases without RF never hold these
+        TB_CUDA(ctx, cudaMalloc(&ctx->d_rf_field, (size_t)tb_halo_count(ctx->nx, ctx->ny) * sizeof(float4)));
+        TB_CUDA(ctx, cudaMalloc(&ctx->d_rf_barrier, 2 * cells * sizeof(float4)));
+    }
+    return tb_launch_pack_rf_fields(ctx, d_rf_ex, d_rf_ey, d_rf_phi, d_wface, (cudaStream_t)stream);
+}
+
 // Reads and clears the device error flag (a synchronising copy).
 static int check_device_flag(tb_ctx *ctx, cudaStream_t s) {
     int flag = 0;
@@ -157,9 +175,10 @@ extern "C" int tb_trace(tb_ctx *ctx, const tb_trace_args *a, int precision, void
         return tb_launch_trace_f64(ctx, a, s);
     }
     if (precision == TB_PRECISION_F32) {
-        if (a->n_phase > 0 || a->record)
-            return tb_fail(ctx, TB_ERR_ARG, "tb_trace: RF clock and record need precision F64");
+        if (a->record) return tb_fail(ctx, TB_ERR_ARG, "tb_trace: record needs precision F64");
         if (!ctx->fields_ready) return tb_fail(ctx, TB_ERR_ARG, "tb_trace: call tb_set_fields first");
+        if (a->n_phase > 0 && (!ctx->rf_ready || ctx->rf_vscale != ctx->vscale))
+            return tb_fail(ctx, TB_ERR_ARG, "tb_trace: FP32 with the RF clock needs tb_set_rf_fields after tb_set_fields");
         return tb_launch_trace_f32(ctx, a, s);
     }
     return tb_fail(ctx, TB_ERR_ARG, "tb_trace: unknown precision %d", precision);

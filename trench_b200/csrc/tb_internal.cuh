@@ -56,7 +56,8 @@ __device__ __forceinline__ tb_fcell tb_pack_cell(double ex, double ey, bool vacu
 }
 
 // Writes the packed value of cell (ix, iy) and its halo copies.
-__device__ __forceinline__ void tb_store_halo(tb_fcell *out, int nx, int ny, int ix, int iy, tb_fcell v) {
+template <typename T>
+__device__ __forceinline__ void tb_store_halo(T *out, int nx, int ny, int ix, int iy, T v) {
     const int P = ny + 2;
     int cs[3], rs[3], nc = 0, nr = 0;
     cs[nc++] = ix + 1;
@@ -91,6 +92,10 @@ struct tb_ctx {
     int tune_threads = 1024;             // FP32 tracer CTA size (tb_set_tuning)
     int tune_ctas_per_sm = 1;            // FP32 tracer CTAs per SM
     int tune_reverse = 0;                // FP32 tracer claims particles from the last index down
+    float4 *d_rf_field = nullptr;        // circuit_rf basis fields (exs, eys, exm, eym) x vac, halo-padded
+    float4 *d_rf_barrier = nullptr;      // (2, nx*ny) per-face wall barrier of each basis potential
+    int rf_ready = 0;
+    double rf_vscale = 0;                // velocity unit the basis fields were packed with
     tb_poisson *poisson = nullptr;        // multigrid hierarchy (tb_poisson_setup)
     char err[512] = {0};
 };
@@ -112,6 +117,8 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s);
 int tb_configure_trace_f32(tb_ctx *ctx);
 int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
                           const double *wface, double vscale, cudaStream_t s);
+int tb_launch_pack_rf_fields(tb_ctx *ctx, const double *rf_ex, const double *rf_ey, const double *rf_phi,
+                             const double *wface, cudaStream_t s);
 
 // Deposits one particle into counts[key] (key = species * cells + cell).  Warp-aggregated:
 // the lanes of the warp that deposit into the same key at this point add once, with

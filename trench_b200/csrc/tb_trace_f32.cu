@@ -44,6 +44,15 @@ struct K32 {
     int bytes;                      // packed field bytes (multiple of 16)
     int pool_off;                   // byte offset of the drain pool in dynamic shared memory, -1 = none
     int reverse;                    // claim particles from the last index down
+    // circuit_rf in flight (kernels with RF = true): the unit-voltage basis fields
+    // (exs, eys, exm, eym) x vac in field units per padded cell, their per-face wall
+    // barriers (substrate basis then mask basis, nx*ny each) and the clock units
+    const float4 *rf_field;
+    const float4 *rf_barrier;
+    float t_phase;                  // fraction of the RF period per unit of step time
+    float t_sec;                    // seconds per unit of step time (dx / vscale)
+    float dt_max;                   // step bound of the in-flight field, in step time
+    float bvs, bvm;                 // largest voltage deltas of the waveform
 };
 
 // 1.0f for a vacuum cell, 0.0f for a solid one, with integer operations only
@@ -107,6 +116,7 @@ __device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mba
 struct LaneState {
     int pid, ix, iy, steps, stop_at, spc;
     float ox, oy, vx, vy, qm;
+    float phase, elapsed;           // circuit_rf: clock as a fraction of the period, seconds in flight
 };
 
 // The four bilinear corners a lane loaded last and their base index (-1 = none).  With
@@ -135,7 +145,21 @@ struct CaseView {
 // field, CFL step, trapezoid update, periodic x, escape, staircase corner, first-face
 // wall entry and barrier reflection; on absorption, escape or the step cap the
 // particle's outputs are written and s.pid becomes -1.
-template <bool SMEM>
+// Linear interpolation of the periodic waveform table at a phase in [0, 1)
+// (trench_rf.py:5-11).
+__device__ __forceinline__ void rf_coefficients(const tb_trace_args &a, float phase, float &vs, float &vm) {
+    const int n = a.n_phase;
+    const float f = phase * (float)n;
+    int i = (int)f;
+    const float w = f - (float)i;
+    i = i >= n ? i - n : i;
+    const int j = i + 1 == n ? 0 : i + 1;
+    const double *wv = a.d_wave;
+    vs = (float)__ldg(wv + 2 * i) * (1.f - w) + (float)__ldg(wv + 2 * j) * w;
+    vm = (float)__ldg(wv + 2 * i + 1) * (1.f - w) + (float)__ldg(wv + 2 * j + 1) * w;
+}
+
+template <bool SMEM, bool RF>
 __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM> &C, LaneState &s, LaneTally &t,
                                               QuadCache &q) {
     const tb_trace_args &a = k.a;
@@ -164,8 +188,39 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
     const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
     const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
-    const float qs = __fdividef(s.qm, fmaxf(sw, 1e-12f));
-    const float ax = qs * sex, ay = qs * sey;
+    float ax, ay, dt;
+    const float speed = sqrtf(s.vx * s.vx + s.vy * s.vy);
+    if (!RF) {
+        const float qs = __fdividef(s.qm, fmaxf(sw, 1e-12f));
+        ax = qs * sex;
+        ay = qs * sey;
+        const float acc = sqrtf(ax * ax + ay * ay);
+        dt = __fdividef(C.cfl, speed + sqrtf(2.f * acc) + C.inv_v);
+    } else {
+        // in-flight RF field (trench_trace.cu:97-110): the basis fields at the same corners
+        // and weights bound the step, and the field is taken at the mid-step clock
+        const float4 b00 = __ldg(k.rf_field + base), b01 = __ldg(k.rf_field + base + 1);
+        const float4 b10 = __ldg(k.rf_field + base + P), b11 = __ldg(k.rf_field + base + P + 1);
+        const float inv_sw = __fdividef(1.f, fmaxf(sw, 1e-12f));
+        const float ex = sex * inv_sw, ey = sey * inv_sw;
+        const float exs = (w00 * b00.x + w10 * b10.x + w01 * b01.x + w11 * b11.x) * inv_sw;
+        const float eys = (w00 * b00.y + w10 * b10.y + w01 * b01.y + w11 * b11.y) * inv_sw;
+        const float exm = (w00 * b00.z + w10 * b10.z + w01 * b01.z + w11 * b11.z) * inv_sw;
+        const float eym = (w00 * b00.w + w10 * b10.w + w01 * b01.w + w11 * b11.w) * inv_sw;
+        const float bx = fabsf(ex) + (k.bvs * fabsf(exs) + k.bvm * fabsf(exm));
+        const float by = fabsf(ey) + (k.bvs * fabsf(eys) + k.bvm * fabsf(eym));
+        const float accel = fabsf(s.qm) * sqrtf(bx * bx + by * by);
+        dt = fminf(k.dt_max, __fdividef(C.cfl, speed + sqrtf(2.f * accel) + C.inv_v));
+        float mid = s.phase + 0.5f * dt * k.t_phase;
+        mid -= floorf(mid);
+        float vs, vm;
+        rf_coefficients(k.a, mid, vs, vm);
+        ax = s.qm * (ex + (vs * exs + vm * exm));
+        ay = s.qm * (ey + (vs * eys + vm * eym));
+        s.phase += dt * k.t_phase;
+        s.phase -= floorf(s.phase);
+        s.elapsed += dt * k.t_sec;
+    }
     // the start cell is the corner on the particle's side of each centre line; its
     // interior flag says every 8-neighbour is vacuum, so a move of < 1 cell cannot
     // touch a wall and the end-cell and corner checks are skipped
@@ -173,9 +228,6 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     const bool near = !(__float_as_uint(start_ey) & 1u);
 
     // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
-    const float speed = sqrtf(s.vx * s.vx + s.vy * s.vy);
-    const float acc = sqrtf(ax * ax + ay * ay);
-    const float dt = __fdividef(C.cfl, speed + sqrtf(2.f * acc) + C.inv_v);
     const float vxn = s.vx + ax * dt, vyn = s.vy + ay * dt;
     const float sx = 0.5f * (s.vx + vxn) * dt, sy = 0.5f * (s.vy + vyn) * dt;
     // a step moves less than one cell, so the new offset lies in (-1, 2): the cell
@@ -237,7 +289,17 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         if (hit && C.barrier) {
             const float4 b = __ldg(k.barrier + ccell);
             // neighbour the particle came from: W/E across an x face, S/N across a y face
-            const float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
+            float dphi = face_x ? (dix > 0 ? b.x : b.y) : (diy_e > 0 ? b.z : b.w);
+            if (RF) {
+                // barrier of the instantaneous potential at the clock after the step
+                // (trench_trace.cu:131-136)
+                float vs, vm;
+                rf_coefficients(a, s.phase, vs, vm);
+                const float4 bs = __ldg(k.rf_barrier + ccell), bm = __ldg(k.rf_barrier + C.cells + ccell);
+                const float ds = face_x ? (dix > 0 ? bs.x : bs.y) : (diy_e > 0 ? bs.z : bs.w);
+                const float dm = face_x ? (dix > 0 ? bm.x : bm.y) : (diy_e > 0 ? bm.z : bm.w);
+                dphi += vs * ds + vm * dm;
+            }
             const float vn = face_x ? vxn : vyn;
             if (0.5f * vn * vn < s.qm * dphi) {
                 // reflect: the normal velocity flips, the position stays at the start point
@@ -278,6 +340,10 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
             a.d_vx[pid] = (double)s.vx * k.vscale;
             a.d_vy[pid] = (double)s.vy * k.vscale;
         }
+        if (RF) {
+            a.d_clock[2 * pid] = (double)s.phase * a.period;
+            a.d_clock[2 * pid + 1] = (double)s.elapsed;
+        }
         s.pid = -1;
     }
 }
@@ -286,11 +352,13 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
 // (struct of arrays over the block's threads): pid; ix | iy << 16 (grids below 32768
 // cells a side, iy >= -1); steps; stop_at | spc << 31; ox, oy, vx, vy, qm.
 constexpr int POOL_WORDS = 9;
+constexpr int POOL_WORDS_RF = 11;   // + phase, elapsed
 #ifndef TB_TAIL_ROUND_STEPS
 #define TB_TAIL_ROUND_STEPS 64
 #endif
 constexpr int TAIL_ROUND_STEPS = TB_TAIL_ROUND_STEPS;
 
+template <bool RF>
 __device__ __forceinline__ void pool_put(uint32_t *P, int T, int q, const LaneState &s) {
     P[0 * T + q] = (uint32_t)s.pid;
     P[1 * T + q] = ((uint32_t)s.ix & 0xffffu) | ((uint32_t)s.iy << 16);
@@ -301,8 +369,13 @@ __device__ __forceinline__ void pool_put(uint32_t *P, int T, int q, const LaneSt
     P[6 * T + q] = __float_as_uint(s.vx);
     P[7 * T + q] = __float_as_uint(s.vy);
     P[8 * T + q] = __float_as_uint(s.qm);
+    if (RF) {
+        P[9 * T + q] = __float_as_uint(s.phase);
+        P[10 * T + q] = __float_as_uint(s.elapsed);
+    }
 }
 
+template <bool RF>
 __device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneState &s) {
     s.pid = (int)P[0 * T + q];
     const uint32_t xy = P[1 * T + q];
@@ -317,6 +390,10 @@ __device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneSt
     s.vx = __uint_as_float(P[6 * T + q]);
     s.vy = __uint_as_float(P[7 * T + q]);
     s.qm = __uint_as_float(P[8 * T + q]);
+    if (RF) {
+        s.phase = __uint_as_float(P[9 * T + q]);
+        s.elapsed = __uint_as_float(P[10 * T + q]);
+    }
 }
 
 // Traces particles of one case with the calling block until the case's queue is
@@ -332,7 +409,7 @@ __device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneSt
 // rounds: the live particles are packed into the first warps, those warps take up
 // to TAIL_ROUND_STEPS steps, and the rest wait at the barrier.  A particle's
 // arithmetic does not depend on its lane, so the results are the same either way.
-template <bool SMEM>
+template <bool SMEM, bool RF>
 __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, uint32_t *pool) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -355,6 +432,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     s.pid = -1;
     s.ix = s.iy = s.steps = s.stop_at = s.spc = 0;
     s.ox = s.oy = s.vx = s.vy = s.qm = 0.f;
+    s.phase = s.elapsed = 0.f;
     LaneTally t = {0u, 0u, 0u, 0u, 0u, 0u};
     QuadCache q;
     q.base = -1;
@@ -398,12 +476,17 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                         s.steps = a.d_steps[pid];
                         s.stop_at = min(a.max_steps, s.steps + a.step_budget);
                         t.steps -= (unsigned)s.steps;   // steps are tallied when the particle stops
+                        if (RF) {
+                            // clock in [0, period) seconds -> fraction of the period
+                            s.phase = fminf(fmaxf((float)(a.d_clock[2 * pid] / a.period), 0.f), ONE_BELOW);
+                            s.elapsed = (float)a.d_clock[2 * pid + 1];
+                        }
                     }
                 }
             }
         }
         if (s.pid < 0) continue;
-        step_particle<SMEM>(k, C, s, t, q);
+        step_particle<SMEM, RF>(k, C, s, t, q);
     }
 
     if (pool != nullptr) {
@@ -413,20 +496,20 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
         for (;;) {
             __syncthreads();
             if (s.pid >= 0) {
-                pool_put(pool, T, atomicAdd(&s_live, 1), s);
+                pool_put<RF>(pool, T, atomicAdd(&s_live, 1), s);
                 s.pid = -1;
             }
             __syncthreads();
             const int live = s_live;
             if (live == 0) break;
-            if ((int)threadIdx.x < live) pool_get(pool, T, threadIdx.x, s);
+            if ((int)threadIdx.x < live) pool_get<RF>(pool, T, threadIdx.x, s);
             q.base = -1;
             __syncthreads();
             if (threadIdx.x == 0) s_live = 0;
             if ((int)(threadIdx.x & ~31u) < live) {  // warp-uniform: this warp holds particles
                 for (int r = 0; r < TAIL_ROUND_STEPS; ++r) {
                     if (__ballot_sync(FULL, s.pid >= 0) == 0u) break;
-                    if (s.pid >= 0) step_particle<SMEM>(k, C, s, t, q);
+                    if (s.pid >= 0) step_particle<SMEM, RF>(k, C, s, t, q);
                 }
             }
         }
@@ -452,7 +535,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     }
 }
 
-template <bool SMEM, int THREADS>
+template <bool SMEM, int THREADS, bool RF>
 __global__ void __launch_bounds__(THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
@@ -465,7 +548,7 @@ __global__ void __launch_bounds__(THREADS, 1) trace_f32_kernel(const __grid_cons
         fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
     }
     uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
-    run_case<SMEM>(k, fieldp, pool);
+    run_case<SMEM, RF>(k, fieldp, pool);
 }
 
 // Many cases in one persistent launch: each CTA repeatedly takes the case with the
@@ -512,7 +595,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1)
             fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
         }
         uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
-        run_case<SMEM>(k, fieldp, pool);
+        run_case<SMEM, false>(k, fieldp, pool);
         __syncthreads();  // every warp is done with this case's field
     }
 }
@@ -540,7 +623,51 @@ __global__ void pack_fields_kernel(int nx, int ny, double scale_e, double scale_
     bar[c] = b;
 }
 
+// Packs the circuit_rf unit-voltage basis fields ((2, nx, ny) each: substrate, mask)
+// into one float4 per halo-padded cell, (exs, eys, exm, eym) x vac x scale_e, and the
+// per-face barriers of the two basis potentials like pack_fields_kernel.
+__global__ void pack_rf_fields_kernel(int nx, int ny, double scale_e, double scale_phi, const uint8_t *vac,
+                                      const double *ex, const double *ey, const double *phi, const double *wface,
+                                      float4 *out, float4 *bar) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cells = nx * ny;
+    if (c >= cells) return;
+    const int ix = c / ny, iy = c - ix * ny;
+    const double v = vac[c] ? scale_e : 0.0;
+    tb_store_halo(out, nx, ny, ix, iy,
+                  make_float4((float)(ex[c] * v), (float)(ey[c] * v), (float)(ex[cells + c] * v),
+                              (float)(ey[cells + c] * v)));
+    for (int b = 0; b < 2; ++b) {
+        float4 r = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (!vac[c] && wface != nullptr) {
+            const double *ph = phi + (size_t)b * cells;
+            const int w = (ix == 0 ? nx - 1 : ix - 1) * ny + iy;
+            const int e = (ix == nx - 1 ? 0 : ix + 1) * ny + iy;
+            const double f = wface[c], pc = ph[c];
+            r.x = (float)(f * (pc - ph[w]) * scale_phi);
+            r.y = (float)(f * (pc - ph[e]) * scale_phi);
+            r.z = iy > 0 ? (float)(f * (pc - ph[c - 1]) * scale_phi) : 0.f;
+            r.w = iy < ny - 1 ? (float)(f * (pc - ph[c + 1]) * scale_phi) : 0.f;
+        }
+        bar[(size_t)b * cells + c] = r;
+    }
+}
+
 }  // namespace
+
+int tb_launch_pack_rf_fields(tb_ctx *ctx, const double *rf_ex, const double *rf_ey, const double *rf_phi,
+                             const double *wface, cudaStream_t s) {
+    const int cells = ctx->nx * ctx->ny;
+    const double vscale = ctx->vscale;
+    const int threads = 256;
+    pack_rf_fields_kernel<<<(cells + threads - 1) / threads, threads, 0, s>>>(
+        ctx->nx, ctx->ny, ctx->dx / (vscale * vscale), 1.0 / (vscale * vscale), ctx->d_vac, rf_ex, rf_ey, rf_phi,
+        wface, ctx->d_rf_field, ctx->d_rf_barrier);
+    TB_CUDA(ctx, cudaGetLastError());
+    ctx->rf_vscale = vscale;
+    ctx->rf_ready = 1;
+    return TB_OK;
+}
 
 int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
                           const double *wface, double vscale, cudaStream_t s) {
@@ -561,12 +688,16 @@ int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const
 // attribute calls; the attribute is per function and device, always this value.
 int tb_configure_trace_f32(tb_ctx *ctx) {
     const int limit = ctx->max_smem - 1024;
-    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      limit));
-    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, 768>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      limit));
-    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      limit));
+#define TB_SMEM_ATTR(T, RF)                                                                                  \
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, T, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                      limit))
+    TB_SMEM_ATTR(1024, false);
+    TB_SMEM_ATTR(768, false);
+    TB_SMEM_ATTR(512, false);
+    TB_SMEM_ATTR(1024, true);
+    TB_SMEM_ATTR(768, true);
+    TB_SMEM_ATTR(512, true);
+#undef TB_SMEM_ATTR
     TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       limit));
     ctx->smem_attr_bytes = limit;
@@ -592,37 +723,36 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     k.pool_off = -1;
     k.reverse = ctx->tune_reverse;
+    k.rf_field = ctx->d_rf_field;
+    k.rf_barrier = ctx->d_rf_barrier;
+    k.t_phase = k.t_sec = k.dt_max = k.bvs = k.bvm = 0.f;
+    if (a->n_phase > 0) {
+        // step time unit dx / vscale: in seconds, in periods, and the in-flight step bound
+        const double unit = ctx->dx / ctx->vscale;
+        k.t_sec = (float)unit;
+        k.t_phase = (float)(unit / a->period);
+        k.dt_max = (float)(a->dt_max / unit);
+        k.bvs = (float)a->bound_vs;
+        k.bvm = (float)a->bound_vm;
+    }
     return k;
 }
 
 // Bytes of the drain pool for a block of `threads`.
-int pool_bytes(int threads) { return POOL_WORDS * 4 * threads; }
+int pool_bytes(int threads, bool rf = false) { return (rf ? POOL_WORDS_RF : POOL_WORDS) * 4 * threads; }
 
 }  // namespace
 
 int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
-    K32 k;
-    k.a = *a;
-    k.nx = ctx->nx;
-    k.ny = ctx->ny;
-    k.dx = ctx->dx;
-    k.vscale = ctx->vscale;
-    k.inv_v = (float)(1.0 / ctx->vscale);
-    k.inv_dx = 1.0 / ctx->dx;
-    k.inv_v64 = 1.0 / ctx->vscale;
-    k.field = ctx->d_field;
-    k.barrier = ctx->d_barrier;
-    k.queue = ctx->d_queue;
-    k.err = ctx->d_err;
-    k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
-    k.reverse = ctx->tune_reverse;
+    K32 k = make_k32(ctx, a);
+    const bool rf = a->n_phase > 0;
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
     const int threads = ctx->tune_threads;
     // the drain pool goes after the field when both fit (without the field it always fits
     // under the default 48 KB)
-    const int pb = pool_bytes(threads);
+    const int pb = pool_bytes(threads, rf);
     size_t shm = smem ? (size_t)k.bytes : 0;
     k.pool_off = -1;
     if (ctx->nx < 65536 && ctx->ny < 32767 && (!smem || k.bytes + pb <= ctx->smem_attr_bytes)) {
@@ -638,8 +768,13 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     if (blocks < 1) blocks = 1;
 #define TB_LAUNCH_F32(T)                                                                        \
     do {                                                                                        \
-        if (smem) trace_f32_kernel<true, T><<<blocks, T, shm, s>>>(k);                         \
-        else trace_f32_kernel<false, T><<<blocks, T, shm, s>>>(k);                             \
+        if (rf) {                                                                               \
+            if (smem) trace_f32_kernel<true, T, true><<<blocks, T, shm, s>>>(k);               \
+            else trace_f32_kernel<false, T, true><<<blocks, T, shm, s>>>(k);                   \
+        } else {                                                                                \
+            if (smem) trace_f32_kernel<true, T, false><<<blocks, T, shm, s>>>(k);              \
+            else trace_f32_kernel<false, T, false><<<blocks, T, shm, s>>>(k);                  \
+        }                                                                                       \
     } while (0)
     if (threads == 512) TB_LAUNCH_F32(512);
     else if (threads == 768) TB_LAUNCH_F32(768);

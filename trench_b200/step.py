@@ -184,6 +184,13 @@ class ChargingCase:
                 self._build_rf(circuit, solver, eps, cond, vac)
             # initial field (trench_charging_2d.py:1198)
             self._potential()
+            if self.rf is not None and precision == "f32":
+                # the FP32 tracer reads the RF basis in its own packed layout, packed once
+                # in the units of the case's field
+                wf = _ptr(self.t_wface) if p.wall_model == "barrier" else None
+                self.ctx.check(_capi.lib().tb_set_rf_fields(
+                    self.ctx.handle, _ptr(self.t_rf["ex"]), _ptr(self.t_rf["ey"]), _ptr(self.t_rf["phi"]), wf,
+                    self._stream()))
 
     # ---- setup helpers -----------------------------------------------------------
     def _build_green(self, rows, green):
@@ -339,8 +346,7 @@ class ChargingCase:
         a.write_state = 0
         precision = self.precision
         if self.rf is not None:
-            # the in-flight RF clock runs on the FP64 kernel
-            precision = "f64"
+            # the in-flight RF clock (precision f32 reads the basis packed at set-up)
             a.d_rf_ex, a.d_rf_ey, a.d_rf_phi = _ptr(self.t_rf["ex"]), _ptr(self.t_rf["ey"]), _ptr(self.t_rf["phi"])
             a.d_wave = _ptr(self.t_rf["wave"])
             a.n_phase = len(self.rf["wave"])

@@ -9,8 +9,9 @@
 
 Inputs are host NumPy arrays (any memory order) or CUDA torch tensors; the
 outputs are new NumPy arrays.  ``precision="f32"`` runs the FP32 shared-memory
-kernel; ``"f64"`` runs the reference-exact FP64 kernel.  Trajectory recording
-and the RF in-flight clock always use the FP64 kernel.  There is no CPU path.
+kernel; ``"f64"`` runs the reference-exact FP64 kernel.  Both carry the RF
+in-flight clock; trajectory recording always uses the FP64 kernel.  There is no
+CPU path.
 """
 import ctypes
 
@@ -156,7 +157,7 @@ class B200Tracer:
         n = len(x)
         nx, ny = self.vac.shape
         f64, dev = torch.float64, self.tdev
-        precision = "f64" if (record is not None or rf is not None) else self.precision
+        precision = "f64" if record is not None else self.precision
         stream = torch.cuda.current_stream(dev)
         sp = ctypes.c_void_p(stream.cuda_stream)
 
@@ -224,6 +225,8 @@ class B200Tracer:
         if precision == "f32" and n:
             self.ctx.check(L.tb_set_fields(ctx.handle, _ptr(EX), _ptr(EY), _ptr(PHI), _ptr(WF),
                                            self.vscale, sp))
+            if rf is not None:
+                ctx.check(L.tb_set_rf_fields(ctx.handle, _ptr(RFX), _ptr(RFY), _ptr(RFP), _ptr(WF), sp))
         cancelled = False
         if stop is None:
             a.step_budget = int(p.max_steps)
