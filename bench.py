@@ -551,6 +551,105 @@ def run_large(args):
     return 0
 
 
+def rf_cycle_workload():
+    """The reference's own circuit_rf benchmark run (its docs/rf_cycle_validation.json):
+    5 nm cells, 120 x 560 grid, trench 80 x 400, conductive mask 60 cells, pillar sides,
+    pulsed 5 kV bias at 400 kHz (duty 0.2, rise 10 ns), 3000 ions + 3000 electrons per
+    batch, max_steps 10000, until_steady with at most 3000 batches.  The circuit waveform
+    over one period comes from the reference's circuit model, run where the reference
+    is available (tests/golden/make_circuit_rf_cycle.py); the charging step reads it.
+    Returns (params, circuit, reference batches, reference seconds)."""
+    from trench_b200.params import Params
+    g = np.load(ROOT / "tests" / "golden" / "circuit_rf_cycle.npz")
+    base = Params()
+    p = replace(base, **{k: v for k, v in json.loads(str(g["params"])).items() if hasattr(base, k)})
+    circuit = {k: np.asarray(g[k]) for k in ("t", "uw", "um", "up", "V1")}
+    return p, circuit, int(g["reference_batches"]), float(g["reference_seconds"])
+
+
+def run_rf_cycle(args):
+    """The circuit_rf run of rf_cycle_workload on one GPU, whole job: batches/s with every
+    batch drawn on the device (Philox; ions at Te/2, stratified launch phases) and replayed
+    from one CUDA graph with the FP32 tracer (value); the same run through the public
+    run() with host injection, setup included (e2e, the measure of the reference's
+    published 222.6 s); and the FP64 tracer on the device-drawn batches for comparison."""
+    import torch
+    from trench_b200 import inject
+    from trench_b200.step import ChargingCase
+    p, circuit, ref_batches, ref_seconds = rf_cycle_workload()
+    published = ref_batches / ref_seconds
+    n = 2 * p.n_per_batch
+
+    def device_run(precision, max_batches, seed):
+        q = replace(p, max_batches=max_batches)
+        case = ChargingCase(q, precision=precision, green="f64", circuit=circuit)
+        inj = inject.DeviceInjector(case, seed=seed)
+        inj(batch=10 ** 6)
+        if precision == "f32":
+            apply_tracer_setting(case, args.tracer_shape, n)
+        torch.cuda.synchronize()
+        clocks = Clocks(torch.cuda.current_device())
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = case.run(injector=inj)
+        e1.record()
+        e1.synchronize()
+        clk = clocks.stop()
+        nb = len(res["hist"]["t"])
+        return case, res, nb, e0.elapsed_time(e1) / 1000.0, clk
+
+    case, res, nb, sec, clk = device_run("f32", p.max_batches, 41)
+    h = res["hist"]
+    tail = slice(max(nb - 10, 0), nb)
+    bottom = [k for k in h if k.startswith("bottom")]
+    f64_case, _, nb64, sec64, _ = device_run("f64", min(300, p.max_batches), 43)
+    del f64_case
+
+    # e2e: the public run() with host injection, construction included
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hcase = ChargingCase(p, precision="f32", green="f64", circuit=circuit)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    hres = hcase.run(rng=np.random.default_rng(p.seed))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    hb = len(hres["hist"]["t"])
+    W = int(p.steady_window)
+    checks = hb // W
+    d2h = sum(k * W * 8 * (hcase.hist_cols + len(hcase.monitor_names)) for k in range(1, checks + 1))
+    line = {"metric": "charging batches/s of the circuit_rf run (reference rf_cycle_validation configuration)",
+            "value": nb / sec, "unit": "batches/s", "n_gpus": 1, "steps": nb, "warmup": 1,
+            "ms_per_step": 1000.0 * sec / nb, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": (nb / sec) / published, "dtype": "f32",
+            "data": "synthetic particles; circuit waveform from the reference's circuit model "
+                    "(tests/golden/circuit_rf_cycle.npz)",
+            "config": {"workload": "circuit_rf run: 5 nm cells, 120x560 grid, trench 80x400, conductive mask 60, "
+                                   "pillar sides, pulsed 5 kV at 400 kHz, 3000 ions + 3000 electrons per batch, "
+                                   "max_steps 10000, until_steady (window 30, hold 2, at most 3000 batches)",
+                       "grid": [case.nx, case.ny], "particles_per_batch": n, "surface_cells": case.m,
+                       "rf_dt_max_s": case.rf["dt_max"], "l2": "not flushed (whole-job run)",
+                       "tracer_shape": list(case.tuning.get("tracer_shape", ())),
+                       "claim_order": case.tuning.get("claim_order")},
+            "batches": nb, "seconds": sec, "converged": bool(res["converged"]),
+            "particles_per_s": nb * n / sec,
+            "lost_fraction_last_10": float(np.mean(h["lost"][tail])),
+            "ratio_i_bottom_last_10": float(np.mean(h["ratio_i_bottom"][tail])),
+            "bottom_potential_last_10_V": {k: float(np.mean(h[k][tail])) for k in bottom},
+            "f64_tracer": {"batches": nb64, "seconds": sec64, "batches_per_s": nb64 / sec64,
+                           "f32_speedup": (nb / sec) / (nb64 / sec64)},
+            "published": {"batches_per_s": published, "batches": ref_batches, "seconds": ref_seconds,
+                          "hardware": "RTX 5070 Ti, reference CUDA FP64 tracer, setup included"},
+            "e2e": {"value": hb / wall, "unit": "batches/s", "batches": hb, "seconds": wall, "setup_s": setup_s,
+                    "loop_batches_per_s": hb / (wall - setup_s), "vs_published": (hb / wall) / published,
+                    "h2d_bytes_per_step": n * (5 * 8 + 1 + 16), "d2h_bytes_per_step": d2h // max(hb, 1),
+                    "note": "ChargingCase construction + run(rng) with host injection (NumPy PCG64) each batch"},
+            "clocks": clk, "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def apply_tracer_setting(case, setting, n):
     """'auto': the autotuner times the launch shapes and claim orders on the loaded batch;
     otherwise '<threads>x<ctas per SM>' with an optional '-reverse' claim order."""
@@ -708,9 +807,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--particles", type=int, default=1 << 19, help="particles per species per batch")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample duration")
-    ap.add_argument("--workload", default="ar8", choices=["ar8", "sweep", "large"],
+    ap.add_argument("--workload", default="ar8", choices=["ar8", "sweep", "large", "rf_cycle"],
                     help="ar8: the AR-8 RF-charging case (default); sweep: many uneven cases per launch; "
-                         "large: the 400x1400 fine-grid case with 2^24 particles per batch")
+                         "large: the 400x1400 fine-grid case with 2^24 particles per batch; rf_cycle: the "
+                         "reference's circuit_rf benchmark run")
     ap.add_argument("--cases", type=int, default=64, help="cases of the sweep workload")
     ap.add_argument("--tracer-shape", default="auto",
                     help="auto (autotuned) or <threads>x<CTAs per SM>[-reverse], e.g. 1024x1-reverse")
@@ -725,6 +825,8 @@ def main():
         return run_sweep(args)
     if args.workload == "large":
         return run_large(args)
+    if args.workload == "rf_cycle":
+        return run_rf_cycle(args)
     p = workload(args.particles)
     if args.impl == "reference":
         return run_reference(args, p)

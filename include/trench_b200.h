@@ -107,8 +107,10 @@ int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, 
  * trace_particles (trench_trace.cu:70-193). */
 int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream);
 
-/* Launch shape of the FP32 tracer on this context: CTA size 512, 768 or 1024 threads
- * and 1 or 2 CTAs per SM (2 only where two shared-memory fields fit on an SM).
+/* Launch shape of the FP32 tracer on this context: CTA size 128, 256, 512, 768 or 1024
+ * threads and 1 or 2 CTAs per SM (2 only where two shared-memory fields fit on an SM).
+ * The launch uses ceil(n / threads) CTAs up to SMs x CTAs per SM, so small CTAs spread
+ * a small batch over more SMs.
  * Chosen by the autotuner (ChargingCase.autotune); default 1024 x 1. */
 int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
 /* Order in which the FP32 tracer's lanes claim particles: 0 in index order
@@ -228,6 +230,12 @@ typedef struct {
                                         batch + *d_counter + 1 (lets a CUDA graph replay a new batch) */
     uint16_t *d_bin_e, *d_bin_a;     /* optional (n_species): table bin of each ion's energy / angle
                                         (0 when that quantity has no table); the adjoint's histories */
+    double *d_clock;                 /* optional circuit_rf clock (2 n_species, 2): launch time, 0 */
+    double period;                   /* RF period (s): each species' launch times are stratified over
+                                        one period, particle k of a species in stratum k
+                                        (trench_rf.py:14-18; the shuffle there only decorrelates
+                                        strata from draws made in sequence, which counter-based
+                                        draws are not) */
 } tb_inject_args;
 
 int tb_inject(tb_ctx *ctx, const tb_inject_args *args, void *stream);

@@ -80,3 +80,31 @@ def test_device_injection_feeds_the_batch_loop(cuda_device):
     case.check()
     h = case.history()
     assert len(h["ratio_i_bottom"]) == 3 and np.all(h["particle_steps"] > 0)
+
+
+def test_device_injection_rf_launch_phases(cuda_device):
+    """circuit_rf: the injector writes stratified launch times (each species covers the
+    period with one particle per stratum, trench_rf.py:14-18), zero flight time, and ions
+    at the Bohm energy Te/2 (trench_charging_2d.py:1135-1139); a run replayed from the
+    device injector accounts for every particle."""
+    from conftest import load_golden
+    from trench_b200.step import ChargingCase
+    g = load_golden("run_rf_taper.npz")
+    circuit = dict(t=g["circuit_t"], uw=g["circuit_uw"], um=g["circuit_um"], up=g["circuit_up"], V1=g["circuit_V1"])
+    p = replace(g["p"], n_per_batch=2000, n_batches=4)
+    case = ChargingCase(p, device=cuda_device, circuit=circuit)
+    n, period = p.n_per_batch, case.rf["period"]
+    inj = inject.DeviceInjector(case, seed=9)
+    inj(0)
+    clock = case.clock[:2 * n].cpu().numpy()
+    assert np.all(clock[:, 1] == 0) and np.all((clock[:, 0] >= 0) & (clock[:, 0] < period))
+    for s in (slice(0, n), slice(n, 2 * n)):
+        np.testing.assert_array_equal(np.sort(np.floor(clock[s, 0] / period * n)), np.arange(n))
+    vx, vy = (t[:n].cpu().numpy() for t in case.X[2:4])
+    m_i = p.ion_mass_amu * AMU
+    np.testing.assert_allclose(0.5 * m_i * vy ** 2 / E_CHARGE, p.electron_temp_eV / 2, rtol=1e-12)
+    assert abs(vx.std() / np.sqrt(p.ion_temp_eV * E_CHARGE / m_i) - 1) < 0.1
+    res = case.run(injector=inject.DeviceInjector(case, seed=10))
+    h = res["hist"]
+    assert len(h["t"]) == p.n_batches and np.all(np.isfinite(res["mean_phi"]))
+    assert np.all(h["particle_steps"] > 0)

@@ -93,6 +93,7 @@ class InjectArgs(ctypes.Structure):
         ("angle_random_sign", ctypes.c_int),
         ("d_counter", _vp),
         ("d_bin_e", _vp), ("d_bin_a", _vp),
+        ("d_clock", _vp), ("period", _dbl),
     ]
 
 

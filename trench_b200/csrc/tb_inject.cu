@@ -89,6 +89,17 @@ __global__ void k_inject(const tb_inject_args a) {
         qm = a.qm_electron;
         spc = 1;
     }
+    if (a.d_clock) {
+        // stratified launch time: stratum k of the species' n, offset by a fifth draw
+        // (counter word 3 with its top bit set, disjoint from the particle counters)
+        uint32_t d[4] = {(uint32_t)i, (uint32_t)(batch & 0xffffffffu), (uint32_t)(batch >> 32),
+                         (uint32_t)(i >> 32) | 0x80000000u};
+        philox4x32_10(d, (uint32_t)(a.seed & 0xffffffffu), (uint32_t)(a.seed >> 32));
+        const long long k = i < n ? i : i - n;
+        const double t = ((double)k + unit(d[0])) * a.period / (double)n;
+        a.d_clock[2 * i] = t < a.period ? t : 0.0;
+        a.d_clock[2 * i + 1] = 0.0;
+    }
     a.d_x[i] = x;
     a.d_y[i] = a.y0;
     a.d_vx[i] = vx;
@@ -115,6 +126,8 @@ extern "C" int tb_inject(tb_ctx *ctx, const tb_inject_args *a, void *stream) {
     if ((a->n_energy > 0 && (!a->d_energy_edges || !a->d_energy_cdf)) ||
         (a->n_angle > 0 && (!a->d_angle_edges || !a->d_angle_cdf)))
         return tb_fail(ctx, TB_ERR_ARG, "tb_inject: a sampling table is missing");
+    if (a->d_clock && !(a->period > 0))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_inject: RF launch times need a positive period");
     if (a->n_energy > 65536 || a->n_angle > 65536)
         return tb_fail(ctx, TB_ERR_ARG, "tb_inject: a table has more than 65536 bins");
     if (a->n_species == 0) return TB_OK;

@@ -694,9 +694,13 @@ int tb_configure_trace_f32(tb_ctx *ctx) {
     TB_SMEM_ATTR(1024, false);
     TB_SMEM_ATTR(768, false);
     TB_SMEM_ATTR(512, false);
+    TB_SMEM_ATTR(256, false);
+    TB_SMEM_ATTR(128, false);
     TB_SMEM_ATTR(1024, true);
     TB_SMEM_ATTR(768, true);
     TB_SMEM_ATTR(512, true);
+    TB_SMEM_ATTR(256, true);
+    TB_SMEM_ATTR(128, true);
 #undef TB_SMEM_ATTR
     TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       limit));
@@ -776,7 +780,9 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
             else trace_f32_kernel<false, T, false><<<blocks, T, shm, s>>>(k);                  \
         }                                                                                       \
     } while (0)
-    if (threads == 512) TB_LAUNCH_F32(512);
+    if (threads == 128) TB_LAUNCH_F32(128);
+    else if (threads == 256) TB_LAUNCH_F32(256);
+    else if (threads == 512) TB_LAUNCH_F32(512);
     else if (threads == 768) TB_LAUNCH_F32(768);
     else TB_LAUNCH_F32(1024);
 #undef TB_LAUNCH_F32
@@ -1049,8 +1055,10 @@ extern "C" int tb_set_claim_order(tb_ctx *ctx, int reverse) {
 
 extern "C" int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm) {
     if (!ctx) return TB_ERR_ARG;
-    if ((threads != 512 && threads != 768 && threads != 1024) || ctas_per_sm < 1 || ctas_per_sm > 2)
-        return tb_fail(ctx, TB_ERR_ARG, "tb_set_tuning: threads must be 512, 768 or 1024 and CTAs per SM 1 or 2");
+    if ((threads != 128 && threads != 256 && threads != 512 && threads != 768 && threads != 1024) ||
+        ctas_per_sm < 1 || ctas_per_sm > 2)
+        return tb_fail(ctx, TB_ERR_ARG,
+                       "tb_set_tuning: threads must be 128, 256, 512, 768 or 1024 and CTAs per SM 1 or 2");
     ctx->tune_threads = threads;
     ctx->tune_ctas_per_sm = ctas_per_sm;
     return TB_OK;

@@ -177,6 +177,9 @@ class DeviceInjector:
         a.ion_mass, a.e_charge = m_i, E_CHARGE
         a.electron_sigma = float(np.sqrt(p.electron_temp_eV * E_CHARGE / M_E))
         a.ion_energy_eV = float(p.ion_energy_eV)
+        if p.field_mode in ("circuit", "circuit_rf") and energy_table is None:
+            # ions start at the plasma potential with the Bohm energy (trench_charging_2d.py:1135-1139)
+            a.ion_energy_eV = float(p.electron_temp_eV) / 2
         a.ion_lateral_sigma = float(np.sqrt(p.ion_temp_eV * E_CHARGE / m_i))
         self._keep = []
         if energy_table is not None:
@@ -188,6 +191,9 @@ class DeviceInjector:
             self._keep += [e, c]
             a.d_angle_edges, a.d_angle_cdf, a.n_angle = _ptr(e), _ptr(c), len(angle_table[0]) - 1
         a.angle_random_sign = int(bool(angle_random_sign))
+        if case.rf is not None:
+            # circuit_rf: stratified launch times over one period into the case's clock
+            a.d_clock, a.period = _ptr(case.clock), float(case.rf["period"])
         self.bin_e = self.bin_a = None
         if bins:
             # table bin of every ion's energy and angle (the adjoint's histories)

@@ -381,7 +381,7 @@ class ChargingCase:
         self.ctx.check(L.tb_step_monitors(self.ctx.handle, ctypes.byref(self._desc), _ptr(self.t_mon_w),
                                           _ptr(self.t_mon_abs), len(self.monitor_names), _ptr(self.qhist), s))
 
-    TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2))
+    TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2), (256, 1), (128, 1))
 
     def autotune_tracer(self, n=None, reps=2):
         """Times the tracer's launch shapes (CTA size, CTAs per SM) and claim orders (index
@@ -629,8 +629,6 @@ class ChargingCase:
         if p.until_steady and start:
             first = steady.history_start(self.history(), probes, self.charge_history())
         converged_at, stopped, check = None, False, None
-        if injector is not None and self.rf is not None:
-            raise ValueError("device injection draws no RF launch phases; circuit_rf runs inject on the host")
         graph = None
         with torch.cuda.device(self.dev):
             for b in range(start, n_max):
