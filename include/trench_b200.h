@@ -93,13 +93,16 @@ int tb_set_fields(tb_ctx *ctx, const double *d_ex, const double *d_ey, const dou
                   const double *d_wface, double vscale, void *stream);
 
 /* Pack the circuit_rf unit-voltage basis fields ((2, nx, ny) Ex, Ey and potential:
- * substrate then mask electrode) for precision F32 with the RF clock: the fields as
- * one float4 per cell and the per-face barrier of each basis potential, in the units
- * of the last tb_set_fields (call it again after a tb_set_fields with another
- * vscale).  The basis is fixed for a case, so one call serves every batch.  Replaces
- * the copies of rf_ex/rf_ey/rf_phi in CudaTracer.__call__ (trench_cuda.py:63-70). */
+ * substrate then mask electrode) and the waveform ((n_phase, 2) voltage deltas over
+ * one period) for precision F32 with the RF clock: the fields as one float4 per cell,
+ * the per-face barrier of each basis potential, in the units of the last
+ * tb_set_fields (call it again after a tb_set_fields with another vscale), and the
+ * waveform as one float4 per table interval.  The basis and waveform are fixed for a
+ * case, so one call serves every batch; tb_trace then requires args->d_wave and
+ * n_phase to be the ones given here.  Replaces the copies of rf_ex/rf_ey/rf_phi/wave
+ * in CudaTracer.__call__ (trench_cuda.py:63-70). */
 int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, const double *d_rf_phi,
-                     const double *d_wface, void *stream);
+                     const double *d_wface, const double *d_wave, int n_phase, void *stream);
 
 /* Trace particles until absorbed, escaped or max_steps; deposit hits into
  * d_counts with integer atomics.  Replaces the chunk loop, kernel launch and host

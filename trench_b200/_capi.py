@@ -128,7 +128,7 @@ SIGNATURES = {
     "tb_last_error": (ctypes.c_char_p, [_vp]),
     "tb_device_info": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "tb_set_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _dbl, _vp]),
-    "tb_set_rf_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp]),
+    "tb_set_rf_fields": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]),
     "tb_trace": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs), ctypes.c_int, _vp]),
     "tb_check": (ctypes.c_int, [_vp, _vp]),
     "tb_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),

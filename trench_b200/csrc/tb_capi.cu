@@ -33,6 +33,7 @@ static int release(tb_ctx *c) {
     cudaFree(c->d_field);
     cudaFree(c->d_barrier);
     cudaFree(c->d_rf_field);
+    cudaFree(c->d_rf_wave);
     cudaFree(c->d_rf_barrier);
     cudaFree(c->d_queue);
     cudaFree(c->d_err);
@@ -113,10 +114,10 @@ extern "C" int tb_set_fields(tb_ctx *ctx, const double *d_ex, const double *d_ey
 }
 
 extern "C" int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, const double *d_rf_phi,
-                                const double *d_wface, void *stream) {
+                                const double *d_wface, const double *d_wave, int n_phase, void *stream) {
     if (!ctx) return TB_ERR_ARG;
-    if (!d_rf_ex || !d_rf_ey || !d_rf_phi)
-        return tb_fail(ctx, TB_ERR_ARG, "tb_set_rf_fields: the basis fields and potentials are required");
+    if (!d_rf_ex || !d_rf_ey || !d_rf_phi || !d_wave || n_phase < 2)
+        return tb_fail(ctx, TB_ERR_ARG, "tb_set_rf_fields: the basis fields, potentials and waveform are required");
     if (!ctx->fields_ready) return tb_fail(ctx, TB_ERR_ARG, "tb_set_rf_fields: call tb_set_fields first");
     TB_CUDA(ctx, cudaSetDevice(ctx->device));
     const size_t cells = (size_t)ctx->nx * ctx->ny;
@@ -125,7 +126,14 @@ extern "C" int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double
         TB_CUDA(ctx, cudaMalloc(&ctx->d_rf_field, (size_t)tb_halo_count(ctx->nx, ctx->ny) * sizeof(float4)));
         TB_CUDA(ctx, cudaMalloc(&ctx->d_rf_barrier, 2 * cells * sizeof(float4)));
     }
-    return tb_launch_pack_rf_fields(ctx, d_rf_ex, d_rf_ey, d_rf_phi, d_wface, (cudaStream_t)stream);
+    if (n_phase > ctx->rf_wave_cap) {
+        TB_CUDA(ctx, cudaFree(ctx->d_rf_wave));
+        ctx->d_rf_wave = nullptr;
+        ctx->rf_wave_cap = 0;
+        TB_CUDA(ctx, cudaMalloc(&ctx->d_rf_wave, (size_t)n_phase * sizeof(float4)));
+        ctx->rf_wave_cap = n_phase;
+    }
+    return tb_launch_pack_rf_fields(ctx, d_rf_ex, d_rf_ey, d_rf_phi, d_wface, d_wave, n_phase, (cudaStream_t)stream);
 }
 
 // Reads and clears the device error flag (a synchronising copy).
@@ -179,6 +187,8 @@ extern "C" int tb_trace(tb_ctx *ctx, const tb_trace_args *a, int precision, void
         if (!ctx->fields_ready) return tb_fail(ctx, TB_ERR_ARG, "tb_trace: call tb_set_fields first");
         if (a->n_phase > 0 && (!ctx->rf_ready || ctx->rf_vscale != ctx->vscale))
             return tb_fail(ctx, TB_ERR_ARG, "tb_trace: FP32 with the RF clock needs tb_set_rf_fields after tb_set_fields");
+        if (a->n_phase > 0 && (a->d_wave != ctx->rf_wave_src || a->n_phase != ctx->rf_n_phase))
+            return tb_fail(ctx, TB_ERR_ARG, "tb_trace: the waveform differs from the one given to tb_set_rf_fields");
         return tb_launch_trace_f32(ctx, a, s);
     }
     return tb_fail(ctx, TB_ERR_ARG, "tb_trace: unknown precision %d", precision);

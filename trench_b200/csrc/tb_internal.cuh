@@ -96,6 +96,10 @@ struct tb_ctx {
     float4 *d_rf_barrier = nullptr;      // (2, nx*ny) per-face wall barrier of each basis potential
     int rf_ready = 0;
     double rf_vscale = 0;                // velocity unit the basis fields were packed with
+    float4 *d_rf_wave = nullptr;         // waveform per table interval: (vs_i, vm_i, vs_i+1 - vs_i, vm_i+1 - vm_i)
+    int rf_wave_cap = 0;                 // intervals allocated
+    int rf_n_phase = 0;                  // intervals packed
+    const double *rf_wave_src = nullptr; // the FP64 waveform they were packed from
     tb_poisson *poisson = nullptr;        // multigrid hierarchy (tb_poisson_setup)
     char err[512] = {0};
 };
@@ -118,7 +122,7 @@ int tb_configure_trace_f32(tb_ctx *ctx);
 int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const double *phi,
                           const double *wface, double vscale, cudaStream_t s);
 int tb_launch_pack_rf_fields(tb_ctx *ctx, const double *rf_ex, const double *rf_ey, const double *rf_phi,
-                             const double *wface, cudaStream_t s);
+                             const double *wface, const double *wave, int n_phase, cudaStream_t s);
 
 // Deposits one particle into counts[key] (key = species * cells + cell).  Warp-aggregated:
 // the lanes of the warp that deposit into the same key at this point add once, with

@@ -46,10 +46,15 @@ struct K32 {
     int reverse;                    // claim particles from the last index down
     // circuit_rf in flight (kernels with RF = true): the unit-voltage basis fields
     // (exs, eys, exm, eym) x vac in field units per padded cell, their per-face wall
-    // barriers (substrate basis then mask basis, nx*ny each) and the clock units
+    // barriers (substrate basis then mask basis, nx*ny each), the waveform per table
+    // interval and the clock units.  The clock is a 32-bit fixed-point fraction of the
+    // period: 2^-32 period resolution, and the wrap at the period is the integer wrap.
     const float4 *rf_field;
     const float4 *rf_barrier;
-    float t_phase;                  // fraction of the RF period per unit of step time
+    const float4 *rf_wave;          // (vs_i, vm_i, vs_i+1 - vs_i, vm_i+1 - vm_i), i < n_phase
+    float t_clock;                  // clock units (2^-32 period) per unit of step time
+    float wave_scale;               // n_phase * 2^-32: clock -> table position
+    int n_phase_m1;
     float t_sec;                    // seconds per unit of step time (dx / vscale)
     float dt_max;                   // step bound of the in-flight field, in step time
     float bvs, bvm;                 // largest voltage deltas of the waveform
@@ -116,7 +121,8 @@ __device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mba
 struct LaneState {
     int pid, ix, iy, steps, stop_at, spc;
     float ox, oy, vx, vy, qm;
-    float phase, elapsed;           // circuit_rf: clock as a fraction of the period, seconds in flight
+    uint32_t clock;                 // circuit_rf: clock in 2^-32 of the period
+    float elapsed;                  // circuit_rf: seconds in flight
 };
 
 // The four bilinear corners a lane loaded last and their base index (-1 = none).  With
@@ -145,18 +151,22 @@ struct CaseView {
 // field, CFL step, trapezoid update, periodic x, escape, staircase corner, first-face
 // wall entry and barrier reflection; on absorption, escape or the step cap the
 // particle's outputs are written and s.pid becomes -1.
-// Linear interpolation of the periodic waveform table at a phase in [0, 1)
-// (trench_rf.py:5-11).
-__device__ __forceinline__ void rf_coefficients(const tb_trace_args &a, float phase, float &vs, float &vm) {
-    const int n = a.n_phase;
-    const float f = phase * (float)n;
-    int i = (int)f;
-    const float w = f - (float)i;
-    i = i >= n ? i - n : i;
-    const int j = i + 1 == n ? 0 : i + 1;
-    const double *wv = a.d_wave;
-    vs = (float)__ldg(wv + 2 * i) * (1.f - w) + (float)__ldg(wv + 2 * j) * w;
-    vm = (float)__ldg(wv + 2 * i + 1) * (1.f - w) + (float)__ldg(wv + 2 * j + 1) * w;
+// Waveform table position of a clock: interval i and the position within it
+// (trench_rf.py:5-11: periodic linear interpolation of n_phase samples; the last
+// interval runs to the first sample).
+__device__ __forceinline__ int rf_interval(const K32 &k, uint32_t clock, float &w) {
+    const float f = (float)clock * k.wave_scale;
+    const int i = min((int)f, k.n_phase_m1);  // a clock just below 2^32 may round up to n
+    w = f - (float)i;
+    return i;
+}
+
+// Voltage deltas (substrate, mask) of the waveform at a clock.
+__device__ __forceinline__ void rf_voltages(const K32 &k, uint32_t clock, float &vs, float &vm) {
+    float w;
+    const float4 e = __ldg(k.rf_wave + rf_interval(k, clock, w));
+    vs = fmaf(w, e.z, e.x);
+    vm = fmaf(w, e.w, e.y);
 }
 
 template <bool SMEM, bool RF>
@@ -198,27 +208,36 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         dt = __fdividef(C.cfl, speed + sqrtf(2.f * acc) + C.inv_v);
     } else {
         // in-flight RF field (trench_trace.cu:97-110): the basis fields at the same corners
-        // and weights bound the step, and the field is taken at the mid-step clock
+        // and weights bound the step, and the field is taken at the mid-step clock.  The
+        // waveform interval of the start clock is loaded before the step is known: a
+        // CFL-limited step is far shorter than an interval, so the mid-step clock is
+        // nearly always in it and the lookup leaves the step's dependency chain.
+        const uint32_t c0 = s.clock;
+        float w0;
+        const int i0 = rf_interval(k, c0, w0);
+        const float4 e0 = __ldg(k.rf_wave + i0);
         const float4 b00 = __ldg(k.rf_field + base), b01 = __ldg(k.rf_field + base + 1);
         const float4 b10 = __ldg(k.rf_field + base + P), b11 = __ldg(k.rf_field + base + P + 1);
+        // weighted sums like the field's; the vacuum normalisation 1/sw is applied once
+        const float sxs = w00 * b00.x + w10 * b10.x + w01 * b01.x + w11 * b11.x;
+        const float sys = w00 * b00.y + w10 * b10.y + w01 * b01.y + w11 * b11.y;
+        const float sxm = w00 * b00.z + w10 * b10.z + w01 * b01.z + w11 * b11.z;
+        const float sym = w00 * b00.w + w10 * b10.w + w01 * b01.w + w11 * b11.w;
         const float inv_sw = __fdividef(1.f, fmaxf(sw, 1e-12f));
-        const float ex = sex * inv_sw, ey = sey * inv_sw;
-        const float exs = (w00 * b00.x + w10 * b10.x + w01 * b01.x + w11 * b11.x) * inv_sw;
-        const float eys = (w00 * b00.y + w10 * b10.y + w01 * b01.y + w11 * b11.y) * inv_sw;
-        const float exm = (w00 * b00.z + w10 * b10.z + w01 * b01.z + w11 * b11.z) * inv_sw;
-        const float eym = (w00 * b00.w + w10 * b10.w + w01 * b01.w + w11 * b11.w) * inv_sw;
-        const float bx = fabsf(ex) + (k.bvs * fabsf(exs) + k.bvm * fabsf(exm));
-        const float by = fabsf(ey) + (k.bvs * fabsf(eys) + k.bvm * fabsf(eym));
-        const float accel = fabsf(s.qm) * sqrtf(bx * bx + by * by);
+        const float bx = fabsf(sex) + (k.bvs * fabsf(sxs) + k.bvm * fabsf(sxm));
+        const float by = fabsf(sey) + (k.bvs * fabsf(sys) + k.bvm * fabsf(sym));
+        const float accel = fabsf(s.qm) * inv_sw * sqrtf(bx * bx + by * by);
         dt = fminf(k.dt_max, __fdividef(C.cfl, speed + sqrtf(2.f * accel) + C.inv_v));
-        float mid = s.phase + 0.5f * dt * k.t_phase;
-        mid -= floorf(mid);
-        float vs, vm;
-        rf_coefficients(k.a, mid, vs, vm);
-        ax = s.qm * (ex + (vs * exs + vm * exm));
-        ay = s.qm * (ey + (vs * eys + vm * eym));
-        s.phase += dt * k.t_phase;
-        s.phase -= floorf(s.phase);
+        const unsigned long long inc = __float2ull_rn(dt * k.t_clock);
+        const uint32_t mid = c0 + (uint32_t)(inc >> 1);
+        float w;
+        const int im = rf_interval(k, mid, w);
+        const float4 e = im == i0 ? e0 : __ldg(k.rf_wave + im);
+        const float vs = fmaf(w, e.z, e.x), vm = fmaf(w, e.w, e.y);
+        const float qs = s.qm * inv_sw;
+        ax = qs * (sex + (vs * sxs + vm * sxm));
+        ay = qs * (sey + (vs * sys + vm * sym));
+        s.clock = c0 + (uint32_t)inc;
         s.elapsed += dt * k.t_sec;
     }
     // the start cell is the corner on the particle's side of each centre line; its
@@ -294,7 +313,7 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
                 // barrier of the instantaneous potential at the clock after the step
                 // (trench_trace.cu:131-136)
                 float vs, vm;
-                rf_coefficients(a, s.phase, vs, vm);
+                rf_voltages(k, s.clock, vs, vm);
                 const float4 bs = __ldg(k.rf_barrier + ccell), bm = __ldg(k.rf_barrier + C.cells + ccell);
                 const float ds = face_x ? (dix > 0 ? bs.x : bs.y) : (diy_e > 0 ? bs.z : bs.w);
                 const float dm = face_x ? (dix > 0 ? bm.x : bm.y) : (diy_e > 0 ? bm.z : bm.w);
@@ -341,7 +360,7 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
             a.d_vy[pid] = (double)s.vy * k.vscale;
         }
         if (RF) {
-            a.d_clock[2 * pid] = (double)s.phase * a.period;
+            a.d_clock[2 * pid] = (double)s.clock * 0x1p-32 * a.period;
             a.d_clock[2 * pid + 1] = (double)s.elapsed;
         }
         s.pid = -1;
@@ -370,7 +389,7 @@ __device__ __forceinline__ void pool_put(uint32_t *P, int T, int q, const LaneSt
     P[7 * T + q] = __float_as_uint(s.vy);
     P[8 * T + q] = __float_as_uint(s.qm);
     if (RF) {
-        P[9 * T + q] = __float_as_uint(s.phase);
+        P[9 * T + q] = s.clock;
         P[10 * T + q] = __float_as_uint(s.elapsed);
     }
 }
@@ -391,7 +410,7 @@ __device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneSt
     s.vy = __uint_as_float(P[7 * T + q]);
     s.qm = __uint_as_float(P[8 * T + q]);
     if (RF) {
-        s.phase = __uint_as_float(P[9 * T + q]);
+        s.clock = P[9 * T + q];
         s.elapsed = __uint_as_float(P[10 * T + q]);
     }
 }
@@ -432,7 +451,8 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     s.pid = -1;
     s.ix = s.iy = s.steps = s.stop_at = s.spc = 0;
     s.ox = s.oy = s.vx = s.vy = s.qm = 0.f;
-    s.phase = s.elapsed = 0.f;
+    s.clock = 0u;
+    s.elapsed = 0.f;
     LaneTally t = {0u, 0u, 0u, 0u, 0u, 0u};
     QuadCache q;
     q.base = -1;
@@ -477,8 +497,9 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                         s.stop_at = min(a.max_steps, s.steps + a.step_budget);
                         t.steps -= (unsigned)s.steps;   // steps are tallied when the particle stops
                         if (RF) {
-                            // clock in [0, period) seconds -> fraction of the period
-                            s.phase = fminf(fmaxf((float)(a.d_clock[2 * pid] / a.period), 0.f), ONE_BELOW);
+                            // clock in [0, period) seconds -> 2^-32 of the period
+                            const double c = a.d_clock[2 * pid] / a.period * 4294967296.0 + 0.5;
+                            s.clock = (uint32_t)(unsigned long long)fmin(fmax(c, 0.0), 4294967295.0);
                             s.elapsed = (float)a.d_clock[2 * pid + 1];
                         }
                     }
@@ -623,6 +644,17 @@ __global__ void pack_fields_kernel(int nx, int ny, double scale_e, double scale_
     bar[c] = b;
 }
 
+// Packs the waveform ((n, 2) voltage deltas per phase sample) into one float4 per
+// table interval: the samples at its start and the differences to the next sample
+// (the last interval runs to the first).
+__global__ void pack_wave_kernel(const double *wave, int n, float4 *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int j = i + 1 == n ? 0 : i + 1;
+    out[i] = make_float4((float)wave[2 * i], (float)wave[2 * i + 1], (float)(wave[2 * j] - wave[2 * i]),
+                         (float)(wave[2 * j + 1] - wave[2 * i + 1]));
+}
+
 // Packs the circuit_rf unit-voltage basis fields ((2, nx, ny) each: substrate, mask)
 // into one float4 per halo-padded cell, (exs, eys, exm, eym) x vac x scale_e, and the
 // per-face barriers of the two basis potentials like pack_fields_kernel.
@@ -656,14 +688,17 @@ __global__ void pack_rf_fields_kernel(int nx, int ny, double scale_e, double sca
 }  // namespace
 
 int tb_launch_pack_rf_fields(tb_ctx *ctx, const double *rf_ex, const double *rf_ey, const double *rf_phi,
-                             const double *wface, cudaStream_t s) {
+                             const double *wface, const double *wave, int n_phase, cudaStream_t s) {
     const int cells = ctx->nx * ctx->ny;
     const double vscale = ctx->vscale;
     const int threads = 256;
     pack_rf_fields_kernel<<<(cells + threads - 1) / threads, threads, 0, s>>>(
         ctx->nx, ctx->ny, ctx->dx / (vscale * vscale), 1.0 / (vscale * vscale), ctx->d_vac, rf_ex, rf_ey, rf_phi,
         wface, ctx->d_rf_field, ctx->d_rf_barrier);
+    pack_wave_kernel<<<(n_phase + threads - 1) / threads, threads, 0, s>>>(wave, n_phase, ctx->d_rf_wave);
     TB_CUDA(ctx, cudaGetLastError());
+    ctx->rf_wave_src = wave;
+    ctx->rf_n_phase = n_phase;
     ctx->rf_vscale = vscale;
     ctx->rf_ready = 1;
     return TB_OK;
@@ -729,12 +764,16 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.reverse = ctx->tune_reverse;
     k.rf_field = ctx->d_rf_field;
     k.rf_barrier = ctx->d_rf_barrier;
-    k.t_phase = k.t_sec = k.dt_max = k.bvs = k.bvm = 0.f;
+    k.rf_wave = ctx->d_rf_wave;
+    k.t_clock = k.wave_scale = k.t_sec = k.dt_max = k.bvs = k.bvm = 0.f;
+    k.n_phase_m1 = 0;
     if (a->n_phase > 0) {
-        // step time unit dx / vscale: in seconds, in periods, and the in-flight step bound
+        // step time unit dx / vscale: in seconds, in clock units, and the in-flight step bound
         const double unit = ctx->dx / ctx->vscale;
         k.t_sec = (float)unit;
-        k.t_phase = (float)(unit / a->period);
+        k.t_clock = (float)(unit / a->period * 4294967296.0);
+        k.wave_scale = (float)(a->n_phase * 0x1p-32);
+        k.n_phase_m1 = a->n_phase - 1;
         k.dt_max = (float)(a->dt_max / unit);
         k.bvs = (float)a->bound_vs;
         k.bvm = (float)a->bound_vm;

@@ -190,7 +190,7 @@ class ChargingCase:
                 wf = _ptr(self.t_wface) if p.wall_model == "barrier" else None
                 self.ctx.check(_capi.lib().tb_set_rf_fields(
                     self.ctx.handle, _ptr(self.t_rf["ex"]), _ptr(self.t_rf["ey"]), _ptr(self.t_rf["phi"]), wf,
-                    self._stream()))
+                    _ptr(self.t_rf["wave"]), len(self.rf["wave"]), self._stream()))
 
     # ---- setup helpers -----------------------------------------------------------
     def _build_green(self, rows, green):

@@ -226,7 +226,8 @@ class B200Tracer:
             self.ctx.check(L.tb_set_fields(ctx.handle, _ptr(EX), _ptr(EY), _ptr(PHI), _ptr(WF),
                                            self.vscale, sp))
             if rf is not None:
-                ctx.check(L.tb_set_rf_fields(ctx.handle, _ptr(RFX), _ptr(RFY), _ptr(RFP), _ptr(WF), sp))
+                ctx.check(L.tb_set_rf_fields(ctx.handle, _ptr(RFX), _ptr(RFY), _ptr(RFP), _ptr(WF), _ptr(WAVE),
+                                             len(rf["wave"]), sp))
         cancelled = False
         if stop is None:
             a.step_budget = int(p.max_steps)
