@@ -650,6 +650,88 @@ def run_rf_cycle(args):
     return 0
 
 
+def standard_workload():
+    """The reference's own CUDA benchmark run (its benchmark_cuda.py, recorded in its
+    docs/cuda_benchmark.json): the standard geometry (5 nm cells, 60 x 200 grid, trench
+    20 x 80, conductive floating mask 60 cells), DC bias, ions 100 eV with a 0.5 eV
+    lateral temperature, Te 3 eV, leakage 1e-15 S, 3000 ions + 3000 electrons per batch,
+    20 batches, seed 1.  Published: CPU 6.045 s, CUDA FP64 0.526 s (median of 3,
+    set-up of the Poisson and leakage operators included, warm-up and plotting excluded)."""
+    from trench_b200.params import Params
+    return replace(Params(), dx=5e-9, nx=60, trench_w=20, trench_d=80, floor_t=10, n_vac=50, mask_t=60,
+                   mask_type="conductor", field_mode="floating", ion_energy_eV=100.0, ion_temp_eV=0.5,
+                   electron_temp_eV=3.0, bias="dc", sigma_s=1e-15, n_batches=20, n_per_batch=3000,
+                   dt_batch=1e-4, cfl=0.35, max_steps=3000, wall_model="barrier", seed=1)
+
+
+def run_standard(args):
+    """The standard-geometry run of standard_workload, timed like the reference's
+    benchmark: ChargingCase construction + run() of 20 batches with host injection,
+    median of 3 after one warm-up run; the oracle's CPU form of the same job beside it."""
+    import torch
+    from oracle import oracle_fields as OF
+    from oracle import oracle_trace as OT
+    from trench_b200 import geometry, inject
+    from trench_b200.step import ChargingCase
+    p = standard_workload()
+    published_cuda, published_cpu = 0.52582550002262, 6.0445344999898225
+    times, setups, res = [], [], None
+    clocks = Clocks(torch.cuda.current_device())
+    for rep in range(4):
+        torch.cuda.synchronize()
+        if rep == 1:
+            clocks.start()
+        t0 = time.perf_counter()
+        case = ChargingCase(p, precision="f32", green="f64")
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        res = case.run(rng=np.random.default_rng(p.seed))
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if rep:
+            times.append(t2 - t0)
+            setups.append(t1 - t0)
+        del case
+    clk = clocks.stop()
+    sec = float(np.median(times))
+    # the oracle's CPU form of the same job: operator set-up, host injection, FP64 C tracer on
+    # all host threads and the FP64 batch update
+    threads = OT.default_threads()
+    t0 = time.perf_counter()
+    solid, mask, _, _ = geometry.build_geometry(p)
+    st = OF.BatchState(p, solid, mask)
+    rng = np.random.default_rng(p.seed)
+    for _ in range(p.n_batches):
+        parts = inject.inject(p, p.n_per_batch, solid.shape[1], rng)
+        st.step(*OT.trace(*parts, st.Ex, st.Ey, ~solid, p, st.barrier(), threads=threads))
+    cpu_s = time.perf_counter() - t0
+    h = res["hist"]
+    n = 2 * p.n_per_batch
+    line = {"metric": "seconds of the reference's CUDA benchmark run (standard geometry, DC, 20 batches)",
+            "value": sec, "unit": "s", "n_gpus": 1, "steps": p.n_batches, "warmup": 1,
+            "ms_per_step": 1000.0 * sec / p.n_batches, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": sec / published_cuda, "dtype": "f32", "data": "synthetic (seeded host injection)",
+            "config": {"workload": "standard geometry: 5 nm cells, 60x200 grid, trench 20x80, floating conductive "
+                                   "mask 60, DC 100 eV ions (0.5 eV lateral), Te 3 eV, sigma_s 1e-15, "
+                                   "3000 ions + 3000 electrons per batch, 20 batches",
+                       "grid": list(solid.shape), "particles_per_batch": n, "timing": "construction + run(), "
+                       "median of 3 after a warm-up run", "l2": "not flushed (whole-job run)"},
+            "setup_s": float(np.median(setups)), "batches_per_s": p.n_batches / sec,
+            "particles_per_s": n * p.n_batches / sec,
+            "published": {"cuda_s": published_cuda, "cpu_s": published_cpu,
+                          "hardware": "RTX 5070 Ti (CUDA FP64 tracer, CPU LU and leakage); CPU model not stated"},
+            "speedup_vs_published_cuda": published_cuda / sec,
+            "ratio_i_bottom_mean": float(np.mean(h["ratio_i_bottom"])),
+            "cpu_baseline": {"value": cpu_s, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": "the whole job: operator set-up, 20 batches of 6000 particles"},
+            "e2e": {"value": sec, "unit": "s", "h2d_bytes_per_step": n * (5 * 8 + 1),
+                    "d2h_bytes_per_step": 0, "note": "the value is already end to end: host injection, "
+                    "construction and result read-back inside the timed region"},
+            "clocks": clk, "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def apply_tracer_setting(case, setting, n):
     """'auto': the autotuner times the launch shapes and claim orders on the loaded batch;
     otherwise '<threads>x<ctas per SM>' with an optional '-reverse' claim order."""
@@ -807,10 +889,10 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--particles", type=int, default=1 << 19, help="particles per species per batch")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="CPU-baseline sample duration")
-    ap.add_argument("--workload", default="ar8", choices=["ar8", "sweep", "large", "rf_cycle"],
+    ap.add_argument("--workload", default="ar8", choices=["ar8", "sweep", "large", "rf_cycle", "standard"],
                     help="ar8: the AR-8 RF-charging case (default); sweep: many uneven cases per launch; "
                          "large: the 400x1400 fine-grid case with 2^24 particles per batch; rf_cycle: the "
-                         "reference's circuit_rf benchmark run")
+                         "reference's circuit_rf benchmark run; standard: the reference's CUDA benchmark run")
     ap.add_argument("--cases", type=int, default=64, help="cases of the sweep workload")
     ap.add_argument("--tracer-shape", default="auto",
                     help="auto (autotuned) or <threads>x<CTAs per SM>[-reverse], e.g. 1024x1-reverse")
@@ -827,6 +909,8 @@ def main():
         return run_large(args)
     if args.workload == "rf_cycle":
         return run_rf_cycle(args)
+    if args.workload == "standard":
+        return run_standard(args)
     p = workload(args.particles)
     if args.impl == "reference":
         return run_reference(args, p)

@@ -184,9 +184,8 @@ class FieldSolver:
         self.schedule_used = (1, 1, 16, 12)
         L = _capi.lib()
         f = lambda a: np.ascontiguousarray(a, dtype=np.float64)
-        ctx.check(L.tb_poisson_setup(ctx.handle, f(d).ctypes.data_as(ctypes.c_void_p),
-                                     f(ke).ctypes.data_as(ctypes.c_void_p), f(kn).ctypes.data_as(ctypes.c_void_p),
-                                     np.ascontiguousarray(fixed).ctypes.data_as(ctypes.c_void_p), self.max_rhs))
+        self._operator = (f(d), f(ke), f(kn), np.ascontiguousarray(fixed))
+        self._setup(self.max_rhs)
         self.levels = L.tb_poisson_levels(ctx.handle)
         self.cond_t = torch.from_numpy(self.cond.ravel()).to(self.dev)
         self.last_iters = 0
@@ -204,6 +203,30 @@ class FieldSolver:
             psi = self._solve_spd(self.w[None, :].clone())[0]
             self.psi = psi
             self.D = float(d[c].sum()) - float(torch.dot(self.w, psi))
+
+    # device bytes per right-hand side and cell: the solver's FP32/FP64 work vectors on
+    # all levels (about 44) plus the FP64 right-hand side, solution and temporaries of
+    # solve_rows (about 48)
+    BYTES_PER_RHS_CELL = 96
+
+    def _setup(self, max_rhs):
+        d, ke, kn, fixed = self._operator
+        ptr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        self.ctx.check(_capi.lib().tb_poisson_setup(self.ctx.handle, ptr(d), ptr(ke), ptr(kn), ptr(fixed),
+                                                    int(max_rhs)))
+        self.max_rhs = int(max_rhs)
+
+    def resize(self, max_rhs):
+        """Right-hand sides per device solve (work vectors are allocated for that many):
+        many for the setup's block solves, where each launch of a small grid is latency-
+        bound and a wider block needs no more launches, few afterwards to hold less memory."""
+        if int(max_rhs) != self.max_rhs:
+            self._setup(max_rhs)
+            self.set_schedule(*self.schedule_used)
+
+    def block_size(self, k, budget_bytes=4 << 30):
+        """Right-hand sides per block for k solves within `budget_bytes` of device memory."""
+        return int(max(1, min(k, budget_bytes // (self.BYTES_PER_RHS_CELL * self.n))))
 
     def _solve_spd(self, bp, x0=None):
         """L x = bp for rows of bp (k, n) on the device (fixed cells must be zero)."""

@@ -94,7 +94,12 @@ class ChargingCase:
                 b = torch.where(self.solver.cond_t[None, :], torch.zeros_like(b), b)
                 self.tuning["poisson"] = {str(k_): v for k_, v in self.solver.autotune(b).items()}
             self.tuning["poisson_schedule"] = self.solver.schedule_used
+            # the m surface Green's solves run as one block where memory allows (a small grid's
+            # solve is launch-bound, so a block of 340 costs about what a block of 64 does)
+            wide = max(self.solver.max_rhs, self.solver.block_size(m))
+            self.solver.resize(wide)
             self._build_green(rows, green)
+            self.solver.resize(max_rhs)
             # leakage (trench_charging_2d.py:768-803)
             self.leak_M = self.leak_h = None
             b0, b1 = geometry.opening_span(solid, p.floor_t)
