@@ -20,6 +20,14 @@
 // Many right-hand sides are solved together: vectors are (nrhs, cells) and
 // every kernel covers all of them in one launch (blockIdx.y = rhs).  Dot products
 // are per-block partial sums added in block order, so a solve is deterministic.
+//
+// Launches: a level's smoothing colour, residual, restriction and prolongation
+// are one launch each, and the coarsest level's sweeps alone are 2 x sweeps x
+// colours launches, so a V-cycle over all levels is about a hundred launches and
+// a small grid's solve is bound by launch latency.  The levels from the first one
+// of at most BOTTOM_MAX_CELLS cells down run instead as one launch, one CTA per
+// right-hand side, with block barriers between the same per-cell steps, so the
+// result is the same bit for bit.
 #include <math.h>
 
 #include <vector>
@@ -29,6 +37,8 @@
 namespace {
 
 constexpr int PT = 256;  // threads per block
+constexpr int BOTTOM_MAX_CELLS = 4096;  // levels this small run inside one fused launch
+constexpr int BOTTOM_THREADS = 512;
 
 struct Level {
     int nx = 0, ny = 0;
@@ -50,6 +60,8 @@ struct tb_poisson {
     double *part = nullptr;                    // (max_rhs, blocks, 2) per-block partial sums
     int part_blocks = 0;
     int pre = 1, post = 1, coarse_sweeps = 16;
+    int bottom = -1;                           // first level run by the fused kernel
+    Level *d_lev = nullptr;                    // device copy of lev
 };
 
 namespace {
@@ -138,20 +150,23 @@ __global__ void k_correct(int n, const float *e, double *x, const double *scal) 
 // red-black checkerboard; with odd nx the periodic wrap would put columns nx-1 and
 // 0 side by side in one colour, so column nx-1 gets colours 2/3 (by row parity) and
 // no two neighbours ever share a colour.
-__global__ void k_smooth(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
-                         float *x, const float *b, int color) {
-    const int n = nx * ny, rhs = blockIdx.y;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
+__device__ __forceinline__ void smooth_at(const Level &L, int rhs, int c, int color) {
+    const int nx = L.nx, ny = L.ny, n = L.n;
     const int ix = c / ny, iy = c - ix * ny;
     const int col = ((nx & 1) && ix == nx - 1) ? 2 + (iy & 1) : ((ix + iy) & 1);
-    if (col != color || fixed[c]) return;
-    float *xr = x + (size_t)rhs * n;
+    if (col != color || L.fixed[c]) return;
+    float *xr = L.x + (size_t)rhs * n;
+    const float *ke = L.ke, *kn = L.kn;
     const int w = wrapx(ix - 1, nx) * ny + iy, e = wrapx(ix + 1, nx) * ny + iy;
-    float s = b[(size_t)rhs * n + c] + ke[c] * xr[e] + ke[w] * xr[w];
+    float s = L.b[(size_t)rhs * n + c] + ke[c] * xr[e] + ke[w] * xr[w];
     if (iy + 1 < ny) s += kn[c] * xr[c + 1];
     if (iy > 0) s += kn[c - 1] * xr[c - 1];
-    xr[c] = s / d[c];
+    xr[c] = s / L.d[c];
+}
+
+__global__ void k_smooth(const Level L, int color) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < L.n) smooth_at(L, blockIdx.y, c, color);
 }
 
 __global__ void k_zero(size_t n, float *x) {
@@ -159,20 +174,19 @@ __global__ void k_zero(size_t n, float *x) {
     if (i < n) x[i] = 0.f;
 }
 
-__global__ void k_resid32(int nx, int ny, const float *d, const float *ke, const float *kn, const uint8_t *fixed,
-                          const float *x, const float *b, float *r) {
-    const int n = nx * ny, rhs = blockIdx.y;
+__device__ __forceinline__ void resid_at(const Level &L, int rhs, int c) {
+    const size_t o = (size_t)rhs * L.n;
+    L.r[o + c] = L.fixed[c] ? 0.f : L.b[o + c] - apply_at(L.d, L.ke, L.kn, L.x + o, L.nx, L.ny, c);
+}
+
+__global__ void k_resid32(const Level L) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    const size_t o = (size_t)rhs * n;
-    r[o + c] = fixed[c] ? 0.f : b[o + c] - apply_at(d, ke, kn, x + o, nx, ny, c);
+    if (c < L.n) resid_at(L, blockIdx.y, c);
 }
 
 // coarse b = sum of the free fine residuals of the 2x2 aggregate
-__global__ void k_restrict(int fnx, int fny, const uint8_t *ffixed, const float *r, int cnx, int cny, float *b) {
-    const int cn = cnx * cny, fn = fnx * fny, rhs = blockIdx.y;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cn) return;
+__device__ __forceinline__ void restrict_at(const Level &F, const Level &C, int rhs, int c) {
+    const int fnx = F.nx, fny = F.ny, cny = C.ny;
     const int I = c / cny, J = c - I * cny;
     float s = 0.f;
     for (int a = 0; a < 2; ++a) {
@@ -182,18 +196,72 @@ __global__ void k_restrict(int fnx, int fny, const uint8_t *ffixed, const float 
             const int j = 2 * J + q;
             if (j >= fny) break;
             const int f = i * fny + j;
-            if (!ffixed[f]) s += r[(size_t)rhs * fn + f];
+            if (!F.fixed[f]) s += F.r[(size_t)rhs * F.n + f];
         }
     }
-    b[(size_t)rhs * cn + c] = s;
+    C.b[(size_t)rhs * C.n + c] = s;
 }
 
-__global__ void k_prolong(int fnx, int fny, const uint8_t *ffixed, float *x, int cnx, int cny, const float *xc) {
-    const int fn = fnx * fny, cn = cnx * cny, rhs = blockIdx.y;
+__global__ void k_restrict(const Level F, const Level C) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < C.n) restrict_at(F, C, blockIdx.y, c);
+}
+
+__device__ __forceinline__ void prolong_at(const Level &F, const Level &C, int rhs, int f) {
+    if (F.fixed[f]) return;
+    const int i = f / F.ny, j = f - i * F.ny;
+    F.x[(size_t)rhs * F.n + f] += C.x[(size_t)rhs * C.n + (i >> 1) * C.ny + (j >> 1)];
+}
+
+__global__ void k_prolong(const Level F, const Level C) {
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= fn || ffixed[f]) return;
-    const int i = f / fny, j = f - i * fny;
-    x[(size_t)rhs * fn + f] += xc[(size_t)rhs * cn + (i >> 1) * cny + (j >> 1)];
+    if (f < F.n) prolong_at(F, C, blockIdx.y, f);
+}
+
+// The V-cycle from level `first` down to the coarsest and back, one CTA per right-hand
+// side (blockIdx.x), the same per-cell steps as the per-level launches in the same
+// order, separated by block barriers (global writes of a block are visible to the
+// block after __syncthreads).
+__global__ void __launch_bounds__(BOTTOM_THREADS) k_vcycle_bottom(const Level *lev, int first, int nlev, int pre,
+                                                                  int post, int coarse_sweeps) {
+    const int rhs = blockIdx.x, t = threadIdx.x, T = blockDim.x;
+    for (int l = first;; ++l) {
+        const Level &L = lev[l];
+        for (int c = t; c < L.n; c += T) L.x[(size_t)rhs * L.n + c] = 0.f;
+        __syncthreads();
+        const int ncol = (L.nx & 1) ? 4 : 2;
+        if (l + 1 == nlev) {
+            for (int dir = 0; dir < 2; ++dir)
+                for (int k = 0; k < coarse_sweeps; ++k)
+                    for (int q = 0; q < ncol; ++q) {
+                        const int color = dir == 0 ? q : ncol - 1 - q;
+                        for (int c = t; c < L.n; c += T) smooth_at(L, rhs, c, color);
+                        __syncthreads();
+                    }
+            break;
+        }
+        for (int k = 0; k < pre; ++k)
+            for (int q = 0; q < ncol; ++q) {
+                for (int c = t; c < L.n; c += T) smooth_at(L, rhs, c, q);
+                __syncthreads();
+            }
+        for (int c = t; c < L.n; c += T) resid_at(L, rhs, c);
+        __syncthreads();
+        const Level &C = lev[l + 1];
+        for (int c = t; c < C.n; c += T) restrict_at(L, C, rhs, c);
+        __syncthreads();
+    }
+    for (int l = nlev - 2; l >= first; --l) {
+        const Level &L = lev[l], &C = lev[l + 1];
+        for (int f = t; f < L.n; f += T) prolong_at(L, C, rhs, f);
+        __syncthreads();
+        const int ncol = (L.nx & 1) ? 4 : 2;
+        for (int k = 0; k < post; ++k)
+            for (int q = 0; q < ncol; ++q) {
+                for (int c = t; c < L.n; c += T) smooth_at(L, rhs, c, ncol - 1 - q);
+                __syncthreads();
+            }
+    }
 }
 
 // q = L p (FP32, fine level); per-block partial sums of p.q into part
@@ -269,13 +337,18 @@ void sweep(const Level &L, int nrhs, bool forward, cudaStream_t s) {
     const int ncol = (L.nx & 1) ? 4 : 2;
     for (int k = 0; k < ncol; ++k) {
         const int color = forward ? k : ncol - 1 - k;
-        k_smooth<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, color);
+        k_smooth<<<g, PT, 0, s>>>(L, color);
     }
 }
 
 // z = M r on the fine level (one symmetric V-cycle); r lives in lev[0].b.
 void vcycle(tb_poisson *ps, int l, int nrhs, cudaStream_t s) {
     Level &L = ps->lev[l];
+    if (l == ps->bottom) {
+        k_vcycle_bottom<<<nrhs, BOTTOM_THREADS, 0, s>>>(ps->d_lev, l, (int)ps->lev.size(), ps->pre, ps->post,
+                                                         ps->coarse_sweeps);
+        return;
+    }
     const size_t tot = (size_t)nrhs * L.n;
     k_zero<<<(unsigned)((tot + PT - 1) / PT), PT, 0, s>>>(tot, L.x);
     const dim3 g = grid_for(L.n, nrhs);
@@ -285,11 +358,11 @@ void vcycle(tb_poisson *ps, int l, int nrhs, cudaStream_t s) {
         return;
     }
     for (int k = 0; k < ps->pre; ++k) sweep(L, nrhs, true, s);
-    k_resid32<<<g, PT, 0, s>>>(L.nx, L.ny, L.d, L.ke, L.kn, L.fixed, L.x, L.b, L.r);
+    k_resid32<<<g, PT, 0, s>>>(L);
     Level &C = ps->lev[l + 1];
-    k_restrict<<<grid_for(C.n, nrhs), PT, 0, s>>>(L.nx, L.ny, L.fixed, L.r, C.nx, C.ny, C.b);
+    k_restrict<<<grid_for(C.n, nrhs), PT, 0, s>>>(L, C);
     vcycle(ps, l + 1, nrhs, s);
-    k_prolong<<<g, PT, 0, s>>>(L.nx, L.ny, L.fixed, L.x, C.nx, C.ny, C.x);
+    k_prolong<<<g, PT, 0, s>>>(L, C);
     for (int k = 0; k < ps->post; ++k) sweep(L, nrhs, false, s);
 }
 
@@ -374,6 +447,7 @@ void tb_poisson_free(tb_poisson *ps) {
     cudaFree(ps->e); cudaFree(ps->pr); cudaFree(ps->pz); cudaFree(ps->pp); cudaFree(ps->pq);
     cudaFree(ps->scal);
     cudaFree(ps->part);
+    cudaFree(ps->d_lev);
     delete ps;
 }
 
@@ -439,10 +513,14 @@ extern "C" int tb_poisson_setup(tb_ctx *ctx, const double *h_diag, const double 
         (rc = upload<float>(ctx, &ps->pr, nullptr, vec)) || (rc = upload<float>(ctx, &ps->pz, nullptr, vec)) ||
         (rc = upload<float>(ctx, &ps->pp, nullptr, vec)) || (rc = upload<float>(ctx, &ps->pq, nullptr, vec)) ||
         (rc = upload<double>(ctx, &ps->scal, nullptr, (size_t)max_rhs * 8)) ||
-        (rc = upload<double>(ctx, &ps->part, nullptr, (size_t)max_rhs * ((n + PT - 1) / PT) * 2))) {
+        (rc = upload<double>(ctx, &ps->part, nullptr, (size_t)max_rhs * ((n + PT - 1) / PT) * 2)) ||
+        (rc = upload<Level>(ctx, &ps->d_lev, ps->lev.data(), ps->lev.size()))) {
         tb_poisson_free(ps);
         return rc;
     }
+    // the fused launch takes over from the first level small enough for one CTA
+    for (int l = 0; l < (int)ps->lev.size(); ++l)
+        if (ps->lev[l].n <= BOTTOM_MAX_CELLS) { ps->bottom = l; break; }
     ctx->poisson = ps;
     return TB_OK;
 }

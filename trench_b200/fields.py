@@ -224,9 +224,14 @@ class FieldSolver:
             self._setup(max_rhs)
             self.set_schedule(*self.schedule_used)
 
-    def block_size(self, k, budget_bytes=4 << 30):
-        """Right-hand sides per block for k solves within `budget_bytes` of device memory."""
-        return int(max(1, min(k, budget_bytes // (self.BYTES_PER_RHS_CELL * self.n))))
+    @classmethod
+    def block_size(cls, k, n, budget_bytes=4 << 30):
+        """Right-hand sides per block for k solves on n cells within `budget_bytes` of
+        device memory."""
+        return int(max(1, min(k, budget_bytes // (cls.BYTES_PER_RHS_CELL * n))))
+
+    # work vectors above this size are released after the set-up's block solves
+    KEEP_BYTES = 256 << 20
 
     def _solve_spd(self, bp, x0=None):
         """L x = bp for rows of bp (k, n) on the device (fixed cells must be zero)."""

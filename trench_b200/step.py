@@ -61,7 +61,12 @@ class ChargingCase:
             eps = geometry.permittivity(solid, mask, p)
             driven = p.field_mode != "floating"
             self.cond, self.eps = cond, eps
-            self.solver = solver = FieldSolver(self.ctx, p, eps, cond, driven, max_rhs=max_rhs)
+            # the m surface Green's solves run as one block where memory allows (a small grid's
+            # solve is launch-bound, so a block of 340 costs about what a block of 64 does); the
+            # work vectors are sized for that block from the start
+            m_surf = int(geometry.surface_cells(solid).sum())
+            wide = max(int(max_rhs), FieldSolver.block_size(m_surf, nx * ny))
+            self.solver = solver = FieldSolver(self.ctx, p, eps, cond, driven, max_rhs=wide)
             # external potential (trench_charging_2d.py:378-394)
             if driven and cond.any():
                 phi_cond = cond.astype(float) * volts["mask"]
@@ -88,18 +93,15 @@ class ChargingCase:
             self.tuning = {}
             if autotune:
                 # the multigrid schedule for the surface Green's solves: timed on a block of them
-                k = min(self.solver.max_rhs, m)
+                k = min(self.solver.max_rhs, m, 64)
                 b = torch.zeros((k, self.n), dtype=torch.float64, device=dev)
                 b[torch.arange(k, device=dev), torch.from_numpy(S[:k]).to(dev)] = p.dx ** 2 / EPS0
                 b = torch.where(self.solver.cond_t[None, :], torch.zeros_like(b), b)
                 self.tuning["poisson"] = {str(k_): v for k_, v in self.solver.autotune(b).items()}
             self.tuning["poisson_schedule"] = self.solver.schedule_used
-            # the m surface Green's solves run as one block where memory allows (a small grid's
-            # solve is launch-bound, so a block of 340 costs about what a block of 64 does)
-            wide = max(self.solver.max_rhs, self.solver.block_size(m))
-            self.solver.resize(wide)
             self._build_green(rows, green)
-            self.solver.resize(max_rhs)
+            if solver.max_rhs * self.n * (FieldSolver.BYTES_PER_RHS_CELL // 2) > FieldSolver.KEEP_BYTES:
+                solver.resize(max_rhs)
             # leakage (trench_charging_2d.py:768-803)
             self.leak_M = self.leak_h = None
             b0, b1 = geometry.opening_span(solid, p.floor_t)
