@@ -249,8 +249,9 @@ int tb_philox_fill(tb_ctx *ctx, unsigned long long seed, unsigned long long batc
 
 /* ---- Case packs: many trench cases in one persistent FP32 launch -----------------
  * A pack groups contexts of one device (different grids allowed).  tb_pack_set_args
- * takes one tb_trace_args per case (FP32 rules of tb_trace; the cases' fields must
- * have been packed) and is synchronous; tb_pack_trace launches one persistent kernel
+ * takes one tb_trace_args per case (FP32 rules of tb_trace, circuit_rf cases
+ * included; the cases' fields, and RF cases' basis, must have been packed) and is
+ * synchronous; tb_pack_trace launches one persistent kernel
  * whose CTAs pick the case with the most unclaimed particles, stage its field in
  * shared memory and trace from its queue, so cases of uneven size share all SMs.
  * reset != 0 first sets status = live, steps = 0 and zeroes counts and totals of every

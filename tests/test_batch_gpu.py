@@ -58,3 +58,34 @@ def test_pack_graph_replay(cuda_device):
     torch.cuda.synchronize()
     for ca, cb in zip(a.cases, b.cases):
         np.testing.assert_array_equal(ca.rho(), cb.rho())
+
+
+def test_pack_with_circuit_rf_case_equals_cases_one_by_one(cuda_device):
+    """A circuit_rf case (in-flight clock, FP32 basis fields) shares the persistent launch
+    with DC cases and gives exactly its single-case result, the others too."""
+    from conftest import load_golden
+    from trench_b200.batch import ChargingBatch
+    from trench_b200.step import ChargingCase
+    g = load_golden("run_rf_taper.npz")
+    circuit = dict(t=g["circuit_t"], uw=g["circuit_uw"], um=g["circuit_um"], up=g["circuit_up"], V1=g["circuit_V1"])
+    ps = [replace(g["p"], n_per_batch=1200)] + small_sweep()[:2]
+    circuits = [circuit, None, None]
+    batch = ChargingBatch(ps, device=cuda_device, max_batches=4, circuits=circuits)
+    singles = [ChargingCase(p, device=cuda_device, precision="f32", max_batches=4, circuit=c)
+               for p, c in zip(ps, circuits)]
+    rngs = [np.random.default_rng(200 + i) for i in range(len(ps))]
+    for _ in range(2):
+        for i, (p, c) in enumerate(zip(ps, singles)):
+            parts = inject.inject(p, p.n_per_batch, c.ny, rngs[i])
+            t0 = None
+            if circuits[i] is not None:
+                t0 = inject.launch_times(rngs[i], 2 * p.n_per_batch, c.rf["period"])
+            batch.load(i, *parts, launch_times=t0)
+            c.load(*parts, launch_times=t0)
+            c.step()
+        batch.step()
+    batch.check()
+    for b, c in zip(batch.cases, singles):
+        c.check()
+        np.testing.assert_array_equal(b.rho(), c.rho())
+        np.testing.assert_array_equal(b.history()["ratio_i_bottom"], c.history()["ratio_i_bottom"])

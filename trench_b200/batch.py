@@ -17,7 +17,6 @@ import torch
 from . import _capi, geometry
 from .params import Params
 from .step import ChargingCase
-from .tracer import _ptr
 
 
 def sweep_params(n_cases, seed=0, base=None):
@@ -49,12 +48,19 @@ def sweep_params(n_cases, seed=0, base=None):
 
 
 class ChargingBatch:
-    def __init__(self, params, device=0, green="f64", max_batches=None):
+    """circuits: optional list with one circuit per case (None for a case without
+    circuit_rf), as ChargingCase takes; RF cases trace with their in-flight clock in the
+    same launch as the others."""
+
+    def __init__(self, params, device=0, green="f64", max_batches=None, circuits=None):
         if not params:
             raise ValueError("a batch needs at least one case")
+        circuits = [None] * len(params) if circuits is None else list(circuits)
+        if len(circuits) != len(params):
+            raise ValueError("one circuit (or None) per case")
         self.dev = torch.device("cuda", int(device))
-        self.cases = [ChargingCase(p, device=device, precision="f32", green=green, max_batches=max_batches)
-                      for p in params]
+        self.cases = [ChargingCase(p, device=device, precision="f32", green=green, max_batches=max_batches,
+                                   circuit=c) for p, c in zip(params, circuits)]
         L = _capi.lib()
         handles = (ctypes.c_void_p * len(self.cases))(*[c.ctx.handle.value for c in self.cases])
         h = ctypes.c_void_p()
@@ -84,8 +90,8 @@ class ChargingBatch:
         except Exception:
             pass
 
-    def load(self, i, x, y, vx, vy, qm, spc, non_blocking=False):
-        self.cases[i].load(x, y, vx, vy, qm, spc, non_blocking=non_blocking)
+    def load(self, i, x, y, vx, vy, qm, spc, non_blocking=False, launch_times=None):
+        self.cases[i].load(x, y, vx, vy, qm, spc, non_blocking=non_blocking, launch_times=launch_times)
         self.n_loaded[i] = len(x)
 
     def _set_args(self):
@@ -93,20 +99,10 @@ class ChargingBatch:
         if self._args_for == key:
             return
         arr = (_capi.TraceArgs * len(self.cases))()
-        for a, c, n in zip(arr, self.cases, self.n_loaded):
-            p = c.p
-            a.n = n
-            a.d_x, a.d_y, a.d_vx, a.d_vy, a.d_qm = (_ptr(t) for t in c.X)
-            a.d_spc = _ptr(c.SPC)
-            bar = p.wall_model == "barrier"
-            a.d_phi, a.d_wface = (_ptr(c.phi), _ptr(c.t_wface)) if bar else (None, None)
-            a.max_steps = a.step_budget = int(p.max_steps)
-            a.cfl = float(p.cfl)
-            a.tapered = int(bool(p.trench_taper_deg or (p.mask_t > 0 and p.mask_taper_deg)))
-            a.d_counts, a.d_totals = _ptr(c.counts), _ptr(c.totals)
-            a.d_status, a.d_steps = _ptr(c.status), _ptr(c.steps)
-            a.d_hit = None
-            a.write_state = 0
+        for i, (c, n) in enumerate(zip(self.cases, self.n_loaded)):
+            # the case's own tracer arguments (fields, barrier, RF clock) for buffer set 0
+            c._fill_args(n, 0)
+            arr[i] = c._args
         self._check(_capi.lib().tb_pack_set_args(self.pack, arr))
         self._args_for = key
 

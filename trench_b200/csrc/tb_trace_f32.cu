@@ -616,7 +616,8 @@ __global__ void __launch_bounds__(F32_THREADS, 1)
             fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
         }
         uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
-        run_case<SMEM, false>(k, fieldp, pool);
+        if (k.a.n_phase > 0) run_case<SMEM, true>(k, fieldp, pool);  // block-uniform: one case per CTA
+        else run_case<SMEM, false>(k, fieldp, pool);
         __syncthreads();  // every warp is done with this case's field
     }
 }
@@ -941,7 +942,11 @@ struct tb_pack {
     int max_particles = 0;
     bool smem = false;
     int pool_off = -1;   // drain pool offset in dynamic shared memory, -1 = none
-    size_t shm = 0;      // dynamic shared memory of the launch
+    size_t shm = 0;      // dynamic shared memory without RF cases
+    bool small_sides = true;
+    int smem_limit = 0;
+    int launch_pool_off = -1;  // pool offset and dynamic shared memory of the launch (tb_pack_set_args)
+    size_t launch_shm = 0;
     int num_sms = 0;
     int ready = 0;
     char err[512] = {0};
@@ -989,10 +994,14 @@ extern "C" int tb_pack_create(tb_pack **out, int n_cases, tb_ctx *const *ctxs) {
     p->shm = p->smem ? (size_t)p->max_bytes : 0;
     bool small_sides = true;
     for (int i = 0; i < n_cases; ++i) small_sides = small_sides && ctxs[i]->nx < 65536 && ctxs[i]->ny < 32767;
+    p->small_sides = small_sides;
+    p->smem_limit = ctxs[0]->smem_attr_bytes;
     if (small_sides && (!p->smem || p->max_bytes + pool_bytes(F32_THREADS) <= ctxs[0]->smem_attr_bytes)) {
         p->pool_off = (int)p->shm;
         p->shm += pool_bytes(F32_THREADS);
     }
+    p->launch_pool_off = p->pool_off;
+    p->launch_shm = p->shm;
     cudaError_t e = cudaSetDevice(dev);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_cases, sizeof(K32) * n_cases);
     if (e == cudaSuccess) e = cudaMalloc(&p->d_queues, sizeof(unsigned long long) * n_cases);
@@ -1027,8 +1036,12 @@ extern "C" int tb_pack_set_args(tb_pack *p, const tb_trace_args *args) {
         const tb_trace_args &a = args[i];
         if (a.n < 0 || a.n > 0x7fffffffLL || !(a.cfl > 0 && a.cfl <= 1) || a.max_steps < 1 || a.step_budget < 1)
             return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: invalid particle count, cfl or step counts");
-        if (a.n_phase > 0 || a.record)
-            return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: the case pack traces in FP32 without RF or record");
+        if (a.record) return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: the case pack traces without record");
+        const tb_ctx *c = p->ctxs[i];
+        if (a.n_phase > 0 && (!c->rf_ready || c->rf_vscale != c->vscale || a.d_wave != c->rf_wave_src ||
+                              a.n_phase != c->rf_n_phase || !a.d_clock || !(a.period > 0) || !(a.dt_max > 0)))
+            return pack_fail(p, TB_ERR_ARG,
+                             "tb_pack_set_args: an RF case needs tb_set_rf_fields with its waveform, and its clock");
         if (!a.d_x || !a.d_y || !a.d_vx || !a.d_vy || !a.d_qm || !a.d_spc || !a.d_counts || !a.d_totals ||
             !a.d_status || !a.d_steps)
             return pack_fail(p, TB_ERR_ARG, "tb_pack_set_args: a required array is missing");
@@ -1039,9 +1052,23 @@ extern "C" int tb_pack_set_args(tb_pack *p, const tb_trace_args *args) {
         ks[i] = make_k32(p->ctxs[i], &a);
         ks[i].queue = p->d_queues + i;
         ks[i].err = p->d_err;
-        ks[i].pool_off = p->pool_off;
         p->max_particles = std::max<int>(p->max_particles, (int)a.n);
     }
+    // RF cases keep two more words per lane in the drain pool
+    bool rf_any = false;
+    for (int i = 0; i < p->n; ++i) rf_any = rf_any || args[i].n_phase > 0;
+    p->launch_pool_off = p->pool_off;
+    p->launch_shm = p->shm;
+    if (rf_any && p->pool_off >= 0) {
+        const size_t base = p->smem ? (size_t)p->max_bytes : 0;
+        if (base + pool_bytes(F32_THREADS, true) <= (size_t)p->smem_limit) {
+            p->launch_shm = base + pool_bytes(F32_THREADS, true);
+        } else {
+            p->launch_pool_off = -1;
+            p->launch_shm = base;
+        }
+    }
+    for (int i = 0; i < p->n; ++i) ks[i].pool_off = p->launch_pool_off;
     cudaError_t e = cudaSetDevice(p->device);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_cases, ks.data(), sizeof(K32) * p->n, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
@@ -1061,9 +1088,9 @@ extern "C" int tb_pack_trace(tb_pack *p, int reset, void *stream) {
         k_pack_reset<<<dim3(blocks, p->n), 256, 0, s>>>(p->d_cases, p->n);
     }
     if (p->smem)
-        trace_f32_batch_kernel<true><<<p->num_sms, F32_THREADS, p->shm, s>>>(p->d_cases, p->n, p->d_err);
+        trace_f32_batch_kernel<true><<<p->num_sms, F32_THREADS, p->launch_shm, s>>>(p->d_cases, p->n, p->d_err);
     else
-        trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, p->shm, s>>>(p->d_cases, p->n, p->d_err);
+        trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, p->launch_shm, s>>>(p->d_cases, p->n, p->d_err);
     e = cudaGetLastError();
     if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
     return TB_OK;
