@@ -327,6 +327,7 @@ def run_b200(args, p):
             dist.barrier()
             dist.destroy_process_group()
         return 0
+    acc = accuracy_measure(case, host[0]) if world == 1 else None
     adj = adjoint_measure() if (args.adjoint and world == 1) else None
     to_steady = steady_measure(p) if (args.steady and world == 1) else None
 
@@ -374,6 +375,7 @@ def run_b200(args, p):
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "batches_per_s": 1000.0 * args.steps * world / e2e_total},
             "device_injection": dinj,
+            "accuracy": acc,
             "adjoint": adj,
             "to_steady": to_steady,
             "gpu_launches": 10 * args.steps,
@@ -784,6 +786,45 @@ def device_injection(case, p, steps):
             "h2d_bytes_per_step": 0, "d2h_bytes_per_step": row.numel() * row.element_size(),
             "note": "inject (Philox, tabulated IED/IAD) + batch step replayed from one CUDA graph; "
                     "history row read back each step"}
+
+
+def accuracy_measure(case, batch):
+    """The FP32 tracer against the FP64 one on one batch of the workload, from the charged
+    state the bench reached: the same particles traced by both kernels from the same
+    charge, each followed by the same charge update.  Per-particle agreement of status and
+    absorbing cell, the bottom ion-flux ratio of the batch (difference in % and in units
+    of its counting noise), and the potential after the update on every cell."""
+    import torch
+    ck = case.checkpoint()
+    n = len(batch[0])
+    case.hit = torch.full((case.capacity,), -1, dtype=torch.int32, device=case.dev)
+    saved = case.precision
+    out = {}
+    try:
+        for prec in ("f32", "f64"):
+            case.restore(ck)
+            case.precision = prec
+            case.hit.fill_(-1)
+            case.load(*batch)
+            case.step(n)
+            torch.cuda.synchronize()
+            out[prec] = dict(status=case.status[:n].cpu().numpy(), hit=case.hit[:n].cpu().numpy(),
+                             ratio=float(case.history()["ratio_i_bottom"][-1]), phi=case.full_potential())
+    finally:
+        case.precision = saved
+        case.hit = None
+        case.restore(ck)
+    a, b = out["f32"], out["f64"]
+    same = (a["status"] == b["status"]) & (a["hit"] == b["hit"])
+    norm = case.p.n_per_batch * (case.b1 - case.b0) / case.nx
+    sigma = np.sqrt(max(b["ratio"] * norm, 1.0)) / norm
+    return {"particles": n, "hit_agreement": float(same.mean()),
+            "ratio_i_bottom": {"f32": a["ratio"], "f64": b["ratio"],
+                               "error_pct": 100.0 * abs(a["ratio"] - b["ratio"]) / max(abs(b["ratio"]), 1e-300),
+                               "error_sigma": abs(a["ratio"] - b["ratio"]) / sigma},
+            "potential_max_abs_diff_V": float(np.abs(a["phi"] - b["phi"]).max()),
+            "note": "one batch of the workload from the charged state, FP32 vs FP64 tracer, same particles "
+                    "and charge; bars: hit agreement >= 0.999, flux error <= 1 %, potential <= 1e-3 V"}
 
 
 def steady_measure(p):
