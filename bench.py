@@ -378,7 +378,8 @@ def run_b200(args, p):
             "accuracy": acc,
             "adjoint": adj,
             "to_steady": to_steady,
-            "gpu_launches": 10 * args.steps,
+            # per step: tracer, fused charge update, Green's GEMV, field, monitors
+            "gpu_launches": 5 * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "wall_s": wall}
     print(json.dumps(line), flush=True)
@@ -548,7 +549,9 @@ def run_large(args):
                          "hbm_peak_gbs": hbm, "hbm_frac_of_measured": achieved / hbm,
                          "note": "algorithmic gather bytes (36 B per particle-step + 28 B per particle) per "
                                  "tracer launch time; the field is L2-resident, no L2 peak is measured"},
-            "e2e": None, "clocks": clk, "gpu_launches": 11 * args.steps}
+            # per step: injection, tracer, deposit, leakage GEMV, finish (m > 1024: unfused charge
+            # update), Green's GEMV, field, monitors
+            "e2e": None, "clocks": clk, "gpu_launches": 8 * args.steps}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -647,7 +650,9 @@ def run_rf_cycle(args):
                     "loop_batches_per_s": hb / (wall - setup_s), "vs_published": (hb / wall) / published,
                     "h2d_bytes_per_step": n * (5 * 8 + 1 + 16), "d2h_bytes_per_step": d2h // max(hb, 1),
                     "note": "ChargingCase construction + run(rng) with host injection (NumPy PCG64) each batch"},
-            "clocks": clk, "gpu_launches": None}
+            "clocks": clk,
+            # per batch: injection, tracer, deposit, leakage GEMV, finish, Green's GEMV, field, monitors
+            "gpu_launches": 8 * nb}
     print(json.dumps(line), flush=True)
     return 0
 
