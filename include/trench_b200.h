@@ -111,10 +111,12 @@ int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, 
 int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream);
 
 /* Launch shape of the FP32 tracer on this context: CTA size 128, 256, 512, 768 or 1024
- * threads and 1 or 2 CTAs per SM (2 only where two shared-memory fields fit on an SM).
- * The launch uses ceil(n / threads) CTAs up to SMs x CTAs per SM, so small CTAs spread
- * a small batch over more SMs.
- * Chosen by the autotuner (ChargingCase.autotune); default 1024 x 1. */
+ * threads and 1 or 2 CTAs per SM (2 only where two shared-memory fields fit on an SM),
+ * or threads = 0: chosen per launch from the batch size (the default).  The launch uses
+ * ceil(n / threads) CTAs up to SMs x CTAs per SM, so small CTAs spread a small batch
+ * over more SMs; the default takes the largest CTA that still gives every SM one (1024
+ * threads for batches of SMs x 768 particles and more, 128 at the least).  Chosen by the
+ * autotuner (ChargingCase.autotune_tracer). */
 int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
 /* Order in which the FP32 tracer's lanes claim particles: 0 in index order
  * (default), 1 from the last index down.  Results do not depend on it; the time

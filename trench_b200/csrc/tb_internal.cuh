@@ -89,7 +89,7 @@ struct tb_ctx {
     int max_smem = 0;                    // opt-in shared memory per block (bytes)
     int smem_attr_bytes = 0;             // dynamic shared memory set on the FP32 tracer
     int smem_per_sm = 0;                 // shared memory of one SM (bytes)
-    int tune_threads = 1024;             // FP32 tracer CTA size (tb_set_tuning)
+    int tune_threads = 0;                // FP32 tracer CTA size (tb_set_tuning), 0 = by batch size
     int tune_ctas_per_sm = 1;            // FP32 tracer CTAs per SM
     int tune_reverse = 0;                // FP32 tracer claims particles from the last index down
     float4 *d_rf_field = nullptr;        // circuit_rf basis fields (exs, eys, exm, eym) x vac, halo-padded

@@ -793,7 +793,12 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
-    const int threads = ctx->tune_threads;
+    int threads = ctx->tune_threads;
+    if (threads == 0) {
+        // by batch size: the largest CTA that still puts one on every SM
+        const long long per_sm_n = (a->n + ctx->num_sms - 1) / std::max(ctx->num_sms, 1);
+        threads = per_sm_n >= 768 ? 1024 : per_sm_n >= 384 ? 512 : per_sm_n >= 192 ? 256 : 128;
+    }
     // the drain pool goes after the field when both fit (without the field it always fits
     // under the default 48 KB)
     const int pb = pool_bytes(threads, rf);
@@ -1121,10 +1126,11 @@ extern "C" int tb_set_claim_order(tb_ctx *ctx, int reverse) {
 
 extern "C" int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm) {
     if (!ctx) return TB_ERR_ARG;
-    if ((threads != 128 && threads != 256 && threads != 512 && threads != 768 && threads != 1024) ||
+    if ((threads != 0 && threads != 128 && threads != 256 && threads != 512 && threads != 768 && threads != 1024) ||
         ctas_per_sm < 1 || ctas_per_sm > 2)
         return tb_fail(ctx, TB_ERR_ARG,
-                       "tb_set_tuning: threads must be 128, 256, 512, 768 or 1024 and CTAs per SM 1 or 2");
+                       "tb_set_tuning: threads must be 0 (by batch size), 128, 256, 512, 768 or 1024 and CTAs "
+                       "per SM 1 or 2");
     ctx->tune_threads = threads;
     ctx->tune_ctas_per_sm = ctas_per_sm;
     return TB_OK;

@@ -324,6 +324,45 @@ class ChargingCase:
         self.SPC[:n].copy_(t, non_blocking=non_blocking)
         self.n_loaded = n
 
+    def _load_staged(self, parts, launch_times=None):
+        """load() for host arrays without waiting for the device: the batch goes into one of
+        two pinned staging buffers and is copied on the stream behind the previous batch's
+        work, so the host draws batch k+1 while the device runs batch k.  A staging buffer
+        is written again only after its previous copy has run (its event)."""
+        n = len(parts[0])
+        if n > self.capacity:
+            raise ValueError(f"{n} particles exceed the case capacity {self.capacity}")
+        if any(len(v) != n for v in parts[1:]):
+            raise ValueError("particle arrays differ in length")
+        if self.rf is not None and (launch_times is None or len(launch_times) != n):
+            raise ValueError("circuit_rf needs one launch time per particle")
+        if not hasattr(self, "_staging"):
+            cap = self.capacity
+            self._staging = [[torch.empty(cap, dtype=torch.float64).pin_memory() for _ in range(5)]
+                             + [torch.empty(cap, dtype=torch.int8).pin_memory(),
+                                torch.empty((cap, 2), dtype=torch.float64).pin_memory()] for _ in range(2)]
+            self._staging_done = [None, None]
+            self._staging_k = 0
+        j = self._staging_k % 2
+        self._staging_k += 1
+        if self._staging_done[j] is not None:
+            self._staging_done[j].synchronize()
+        buf = self._staging[j]
+        for dst, src in zip(buf[:5], parts[:5]):
+            np.copyto(dst[:n].numpy(), src, casting="same_kind")
+        np.copyto(buf[5][:n].numpy(), parts[5], casting="unsafe")
+        for dst, src in zip(self.X + [self.SPC], buf[:6]):
+            dst[:n].copy_(src[:n], non_blocking=True)
+        if self.rf is not None:
+            clk = buf[6][:n].numpy()
+            clk[:, 0] = np.asarray(launch_times, dtype=np.float64) % self.rf["period"]
+            clk[:, 1] = 0.0
+            self.clock[:n].copy_(buf[6][:n], non_blocking=True)
+        ev = torch.cuda.Event()
+        ev.record(torch.cuda.current_stream(self.dev))
+        self._staging_done[j] = ev
+        self.n_loaded = n
+
     def add_input_buffer(self):
         """A second set of particle input buffers, so the next batch can be copied in while
         the current one runs (see HostPipeline)."""
@@ -664,7 +703,7 @@ class ChargingCase:
                     if phase_rng is not None:
                         t0 = np.concatenate([launch_times(phase_rng, p.n_per_batch, self.rf["period"])
                                              for _ in range(2)])
-                    self.load(*parts, launch_times=t0)
+                    self._load_staged(parts, launch_times=t0)
                     self.step()
                 if log is not None and ((b + 1) % 10 == 0 or b == 0):
                     log(f"[{b + 1}/{n_max}]")
