@@ -113,3 +113,19 @@ def test_histogram_tables():
     assert c[0] == 0 and c[-1] == 1 and np.all(np.diff(c) >= 0)
     # the median of the symmetric bimodal density lies between the peaks
     assert 60 < np.interp(0.5, c, e) < 120
+
+
+@pytest.mark.parametrize("change", [dict(bias="dc"), dict(top_bc="neumann"), dict(rf_time_steps=0),
+                                    dict(dt_batch=1e-12)])
+def test_invalid_rf_cycle_settings_are_rejected(change):
+    """circuit_rf needs the RF bias, a Dirichlet top, at least 16 clock steps per period and
+    batches of at least one period (tests/test_rf_cycle.py:159-165)."""
+    from trench_b200.fields import field_voltages
+    settings = dict(nx=20, trench_w=6, trench_d=12, floor_t=4, mask_t=4, n_vac=8, field_mode="circuit_rf",
+                    bias="rf", side_bc="pillar", rf_freq=2.5e9, sigma_s=0)
+    p = replace(Params(), **{**settings, **change})
+    solid, mask, _, _ = geometry.build_geometry(p)
+    t = np.arange(256) * 4e-10 / 256
+    circuit = dict(t=t, uw=-80 + 0 * t, um=-40 + 0 * t, up=10 + 0 * t, V1=50 + 0 * t)
+    with pytest.raises(ValueError):
+        field_voltages(p, mask, circuit)

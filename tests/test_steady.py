@@ -43,3 +43,18 @@ def test_history_start_skips_missing_values():
     mon = {"left": np.array([1.0, np.nan, 2.0, 3.0])}
     assert steady.history_start(hist, ["a"], mon) == 2
     assert steady.history_start({"a": np.ones(3)}, ["a"], {"left": np.ones(3)}) == 0
+
+
+def test_potential_scale_is_the_charging_potential_not_the_rf_bias():
+    """Under the RF circuit the potentials are compared relative to the external ones, so a
+    large bias does not widen the tolerance (tests/test_rf_cycle.py:148-156)."""
+    from dataclasses import replace
+    from trench_b200.params import Params
+    p = replace(Params(), steady_window=30)
+    charging = np.arange(60) * 0.1
+    hist = {"wall": charging - 1000}
+    assert steady.check_steady(hist, ["wall"], p)[0]          # the bias alone would pass it
+    correct = steady.check_steady(hist, ["wall"], p, dict(wall=-1000))
+    no_bias = steady.check_steady({"wall": charging}, ["wall"], p, dict(wall=0))
+    assert not correct[0]
+    np.testing.assert_allclose(correct[2:], no_bias[2:], rtol=1e-12)
