@@ -415,6 +415,8 @@ def run_sweep(args):
         batch.replay()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
     torch.cuda.synchronize()
+    clocks = Clocks(0)
+    clocks.start()
     ms = []
     for _ in range(args.steps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -424,6 +426,7 @@ def run_sweep(args):
         flush.zero_()
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
     batch.check()
     steps_per_batch = sum(c.history()["particle_steps"][-1] for c in batch.cases)
     line = {"metric": METRIC, "value": total / (np.mean(ms) / 1000.0), "unit": "particles/s", "n_gpus": 1,
@@ -434,7 +437,11 @@ def run_sweep(args):
                                    "mask conductive/dielectric, particles/species log-uniform 2^15-2^17, "
                                    "bimodal IED separation 30-150 eV", "cases": len(ps),
                        "particles_per_batch": total, "setup_s": setup_s},
-            "batches_per_s": 1000.0 / float(np.mean(ms)), "particle_steps_per_batch": float(steps_per_batch)}
+            "batches_per_s": 1000.0 / float(np.mean(ms)), "particle_steps_per_batch": float(steps_per_batch),
+            "clocks": clk,
+            # per step: the pack's reset and tracer launches, then per case the fused charge update
+            # (surface cells <= 1024 in every sweep case), Green's GEMV and field
+            "gpu_launches": (2 + 3 * len(ps)) * args.steps}
     print(json.dumps(line), flush=True)
     return 0
 
