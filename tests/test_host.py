@@ -129,3 +129,16 @@ def test_invalid_rf_cycle_settings_are_rejected(change):
     circuit = dict(t=t, uw=-80 + 0 * t, um=-40 + 0 * t, up=10 + 0 * t, V1=50 + 0 * t)
     with pytest.raises(ValueError):
         field_voltages(p, mask, circuit)
+
+
+def test_circuit_phase_is_periodic_and_gauge_invariant():
+    """tests/test_features.py:97-104: electrode voltages relative to the plasma, periodic in phase."""
+    from trench_b200.fields import circuit_voltages
+    c = dict(t=np.arange(4) * 1e-8, uw=np.array([-80.0, -100.0, -80.0, -60.0]),
+             um=np.array([-40.0, -50.0, -40.0, -30.0]), up=np.full(4, 10.0), V1=np.array([50.0, 60.0, 50.0, 40.0]))
+    v = circuit_voltages(c, 45)
+    assert v == dict(substrate=-100, mask=-55, top=0, sheath=55)
+    assert circuit_voltages(c, 405) == v
+    for k in ("uw", "um", "up"):
+        c[k] = c[k] + 123
+    assert circuit_voltages(c, 45) == v

@@ -73,3 +73,30 @@ def test_probe_requires_a_steady_result(cuda_device):
     stop = threading.Event()
     stop.set()
     assert probe_vertical_ions(res, log=None, stop=stop, device=cuda_device)["cancelled"]
+
+
+def test_full_cycle_probe_uses_identical_phases_and_preserves_charge(cuda_device):
+    """circuit_rf probe (tests/test_rf_cycle.py:176-193, without the plots): the charged and
+    uncharged beams start at the same stratified phases, the clock runs in flight, the
+    charge is untouched and every ion is accounted for."""
+    from trench_b200.probe import probe_vertical_ions
+    p = replace(Params(), nx=20, trench_w=6, trench_d=12, floor_t=4, mask_t=4, n_vac=8, field_mode="circuit_rf",
+                bias="rf", side_bc="pillar", rf_freq=2.5e9, sigma_s=0, probe_ions=128, probe_trajectories=8,
+                max_steps=1000, probe_energy_eV=1.5)
+    period = 4e-10
+    t = np.arange(256) * period / 256
+    up = 10 + 2 * np.cos(2 * np.pi * t / period)
+    circuit = dict(t=t, up=up, uw=-80 - 35 * np.sin(2 * np.pi * t / period) + up,
+                   um=-40 - 17.5 * np.sin(2 * np.pi * t / period) + up, V1=50 + 0 * t)
+    solid, mask, i0, _ = geometry.build_geometry(p)
+    rho = np.zeros(solid.shape)
+    rho[i0 - 1, p.floor_t:p.floor_t + p.trench_d] = 3e6
+    res = dict(params=asdict(p), solid=solid, mask=mask, rho_raw=rho, t_conv=1e-3, stopped=False, circuit=circuit)
+    before = rho.copy()
+    d = probe_vertical_ions(res, log=None, device=cuda_device)
+    assert d["rf_cycle"]
+    np.testing.assert_array_equal(d["charged"]["launch_phase"], d["uncharged"]["launch_phase"])
+    assert np.max(np.abs(d["charged"]["final_phase"] - d["charged"]["launch_phase"])) > 1
+    np.testing.assert_array_equal(res["rho_raw"], before)
+    for label in ("charged", "uncharged"):
+        assert d[label]["hits"].sum() + d[label]["escaped"] + d[label]["lost"] == p.probe_ions
