@@ -142,3 +142,53 @@ def test_circuit_phase_is_periodic_and_gauge_invariant():
     for k in ("uw", "um", "up"):
         c[k] = c[k] + 123
     assert circuit_voltages(c, 45) == v
+
+
+def _saved_run():
+    from dataclasses import asdict
+    g = load_golden("run_floating_leak.npz")
+    p = g["p"]
+    hist = {k[5:]: g[k] for k in g if k.startswith("hist_")}
+    return p, dict(params=asdict(p), rho_raw=g["rho_raw"], hist=hist, solid=g["solid"], mask=g["mask"],
+                   checkpoint=dict(version=1, batches_completed=len(hist["t"]), steady_n_ok=0))
+
+
+@pytest.mark.parametrize("changes", [dict(trench_offset=1), dict(dt_batch=2e-4), dict(flux=2e20), dict(rf_volt=200),
+                                     dict(n_per_batch=256), dict(seed=2)])
+def test_resume_rejects_changes_to_physics_and_particles(changes):
+    """tests/test_resume.py:164-170: a resumed run keeps the saved geometry, physics and particles."""
+    from trench_b200.step import validate_resume
+    p, res = _saved_run()
+    with pytest.raises(ValueError, match="keep the geometry"):
+        validate_resume(res, replace(p, **changes))
+
+
+def test_resume_accepts_loop_settings_and_display_rounding():
+    from trench_b200.step import validate_resume
+    p, res = _saved_run()
+    n = len(res["hist"]["t"])
+    assert validate_resume(res, replace(p, n_batches=5, steady_rtol=0.01)) == n
+    assert validate_resume(res, replace(p, dt_batch=p.dt_batch * (1 + 1e-12), dx=p.dx * (1 - 1e-12))) == n
+
+
+def test_resume_rejects_invalid_cap_history_and_checkpoint():
+    """tests/test_resume.py:181-193."""
+    import copy
+    from trench_b200.step import validate_resume
+    p, res = _saved_run()
+    n = len(res["hist"]["t"])
+    with pytest.raises(ValueError, match="whole run"):
+        validate_resume(res, replace(p, until_steady=True, max_batches=n))
+    damaged = copy.deepcopy(res)
+    damaged["hist"]["t"] = damaged["hist"]["t"].copy()
+    damaged["hist"]["t"][-1] += p.dt_batch
+    with pytest.raises(ValueError, match="continuous history"):
+        validate_resume(damaged, p)
+    damaged = copy.deepcopy(res)
+    damaged["checkpoint"]["batches_completed"] = n - 1
+    with pytest.raises(ValueError, match="batch count"):
+        validate_resume(damaged, p)
+    damaged = copy.deepcopy(res)
+    damaged["rho_raw"] = damaged["rho_raw"][:-1]
+    with pytest.raises(ValueError, match="wrong shape"):
+        validate_resume(damaged, p)

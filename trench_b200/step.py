@@ -29,6 +29,64 @@ from .tracer import DEFAULT_VSCALE, Context, _ptr
 
 HIST_SCALARS = ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost", "leak", "particle_steps")
 CHECKPOINT_VERSION = 1
+# settings a resumed run may change; everything else must equal the saved run's
+# (trench_charging_2d.py:951-954; rf_phase too under circuit_rf, where it only moves the display)
+RESUME_EDITABLE = frozenset(("until_steady", "n_batches", "max_batches", "steady_window", "steady_rtol",
+                             "steady_charge_rtol", "steady_charge_atol", "steady_hold", "backend", "cuda_device",
+                             "probe_ions", "probe_energy_eV", "probe_trajectories"))
+
+
+def validate_resume(res, p):
+    """Checks a saved result against the settings of the run that continues it and returns
+    the number of batches it holds (the rules of trench_charging_2d.py:959-1007):
+    geometry, physics and particle settings unchanged (floats within 1e-9 relative, the
+    round trip of a display unit), the same solid and mask, a finite charge of the grid's
+    shape, a history with one entry per batch at the batch times, a checkpoint of this
+    version holding that many batches and a valid steady streak, and a batch cap beyond
+    the saved batches (until_steady) or at least one more batch.  Raises ValueError."""
+    params = dict(res.get("params") or {})
+    editable = RESUME_EDITABLE | ({"rf_phase"} if params.get("field_mode") == "circuit_rf" else set())
+    changed = []
+    for k, v in params.items():
+        if k in editable or not hasattr(p, k):
+            continue
+        entered = getattr(p, k)
+        same = (bool(np.isclose(entered, v, rtol=1e-9, atol=0)) if isinstance(v, float) and
+                isinstance(entered, (int, float)) else entered == v)
+        if not same:
+            changed.append(k)
+    if changed:
+        raise ValueError("a resumed run must keep the geometry, physics and particle settings of the saved "
+                         "run: " + ", ".join(changed))
+    solid, mask, _, _ = geometry.build_geometry(p)
+    if ("solid" in res and not np.array_equal(res["solid"], solid)) or (
+            "mask" in res and not np.array_equal(res["mask"], mask)):
+        raise ValueError("the saved result's geometry differs from this run's")
+    rho = np.asarray(res["rho_raw"])
+    if rho.shape != solid.shape or not np.isfinite(rho).all():
+        raise ValueError("the saved charge has the wrong shape or non-finite values")
+    dt = float(params.get("dt_batch", p.dt_batch))
+    t = np.asarray((res.get("hist") or {}).get("t", []))
+    n = t.size if t.ndim == 1 else 0
+    if n == 0 or not np.isfinite(t).all() or not np.allclose(t, np.arange(1, n + 1) * dt, rtol=1e-10,
+                                                               atol=dt * 1e-8):
+        raise ValueError("resuming needs a continuous history with the batch times")
+    for family in ("hist", "charge_hist", "charge_monitor_hist"):
+        for name, values in (res.get(family) or {}).items():
+            a = np.asarray(values)
+            if a.ndim != 1 or len(a) != n or np.isinf(a).any():
+                raise ValueError(f"a saved history has the wrong length or infinite values: {family}/{name}")
+    ck = res.get("checkpoint")
+    if ck and (ck.get("version") != CHECKPOINT_VERSION or ck.get("batches_completed") != n):
+        raise ValueError("the saved checkpoint's version or batch count does not match its history")
+    hold = int(params.get("steady_hold", p.steady_hold))
+    if ck and (not isinstance(ck.get("steady_n_ok"), (int, np.integer)) or not 0 <= ck["steady_n_ok"] <= hold):
+        raise ValueError("the saved steady-state streak is invalid")
+    if p.until_steady and p.max_batches <= n:
+        raise ValueError(f"max_batches counts the whole run: raise it above the {n} saved batches")
+    if not p.until_steady and p.n_batches < 1:
+        raise ValueError("a resumed run needs at least one more batch")
+    return n
 
 
 class ChargingCase:
@@ -640,6 +698,7 @@ class ChargingCase:
         phase_rng = None
         n_ok = 0
         if resume is not None:
+            validate_resume(resume, p)
             self.restore(resume)
             ck = resume.get("checkpoint") or {}
             if rng is None and ck.get("rng_state"):
