@@ -400,3 +400,29 @@ def test_autotuners_pick_a_shape_and_keep_results(case_cls):
     assert "poisson_schedule" in tuned.tuning and "tracer_shape" in tuned.tuning
     assert tuned.tuning["claim_order"] in ("index", "reverse")
     assert _capi.lib().tb_set_claim_order(tuned.ctx.handle, 2) == _capi.TB_ERR_ARG
+
+
+class _StopAfter:
+    """A stop flag that is raised after `k` checks (the loop checks it before each batch)."""
+
+    def __init__(self, k):
+        self.k = k
+
+    def is_set(self):
+        self.k -= 1
+        return self.k < 0
+
+
+def test_stop_during_resume_keeps_the_last_batch_and_can_resume_again(case_cls):
+    """tests/test_resume.py:196-206: a resumed run stopped between batches returns a result that
+    resumes again, and the pieces together equal the continuous run bit for bit."""
+    p = replace(Params(), nx=30, trench_w=10, trench_d=20, floor_t=5, mask_t=6, n_vac=12, bias="dc",
+                sigma_s=1e-14, n_per_batch=800, n_batches=3, seed=6)
+    full = case_cls(replace(p, n_batches=8), max_batches=10).run()
+    part = case_cls(p, max_batches=10).run()
+    interrupted = case_cls(p, max_batches=10).run(resume=part, stop=_StopAfter(1))
+    assert interrupted["stopped"] and len(interrupted["hist"]["t"]) == 4
+    resumed = case_cls(replace(p, n_batches=4), max_batches=10).run(resume=interrupted)
+    np.testing.assert_array_equal(resumed["rho_raw"], full["rho_raw"])
+    for k in full["hist"]:
+        np.testing.assert_array_equal(resumed["hist"][k], full["hist"][k])
