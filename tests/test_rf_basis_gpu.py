@@ -83,3 +83,17 @@ def test_display_phase_does_not_change_the_charge(cuda_device):
         np.testing.assert_array_equal(a["hist"][key], b["hist"][key])
     assert np.max(np.abs(a["phi"] - b["phi"])) > 10
     np.testing.assert_allclose(a["mean_phi"][a["mask"]], -40, atol=1e-9)
+
+
+def test_rf_resume_equals_continuous_run(cuda_device):
+    """circuit_rf split and resumed (particle and launch-phase generator states carried in the
+    checkpoint) equals the continuous run bit for bit (tests/test_resume.py:61-89)."""
+    from trench_b200.step import ChargingCase
+    p = small_rf_params(n_batches=4, n_per_batch=256)
+    c = waveform()
+    full = ChargingCase(p, device=cuda_device, circuit=c, max_batches=6).run()
+    part = ChargingCase(replace(p, n_batches=2), device=cuda_device, circuit=c, max_batches=6).run()
+    resumed = ChargingCase(replace(p, n_batches=2), device=cuda_device, circuit=c, max_batches=6).run(resume=part)
+    np.testing.assert_array_equal(resumed["rho_raw"], full["rho_raw"])
+    for k in full["hist"]:
+        np.testing.assert_array_equal(resumed["hist"][k], full["hist"][k])
