@@ -27,7 +27,7 @@ def case_cls(cuda_device):
 @pytest.mark.parametrize("name", ["floating", "fixed", "dielectric", "cfg2"])
 def test_solver_matches_reference_lu(case_cls, name):
     """Potential of a given charge: multigrid vs the reference's LU within 1e-9 V
-    (north-star bar 1e-3 V); leakage operator and conductor response likewise."""
+    (the accuracy bar is 1e-3 V); leakage operator and conductor response likewise."""
     g = load_golden(f"fields_{name}.npz")
     p = g["p"]
     case = case_cls(replace(p, n_batches=1), green="f64")
