@@ -1,4 +1,4 @@
-"""bench.py's reference arm on the CPU: one JSON line with the keys the driver reads, on
+"""bench.py's reference arm on the CPU: one JSON line with the keys of the bench contract, on
 the same metric, unit and workload as the B200 arm; ranks other than 0 print nothing."""
 import json
 import os
