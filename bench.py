@@ -589,6 +589,9 @@ def run_rf_cycle(args):
     from trench_b200 import inject
     from trench_b200.step import ChargingCase
     p, circuit, ref_batches, ref_seconds = rf_cycle_workload()
+    if args.rf_batches:
+        # a shorter run (profiling): the batch cap of every leg
+        p = replace(p, max_batches=min(p.max_batches, args.rf_batches))
     published = ref_batches / ref_seconds
     n = 2 * p.n_per_batch
 
@@ -947,6 +950,8 @@ def main():
                          "large: the 400x1400 fine-grid case with 2^24 particles per batch; rf_cycle: the "
                          "reference's circuit_rf benchmark run; standard: the reference's CUDA benchmark run")
     ap.add_argument("--cases", type=int, default=64, help="cases of the sweep workload")
+    ap.add_argument("--rf-batches", type=int, default=0,
+                    help="rf_cycle workload: cap every leg at this many batches (0: the full 3000)")
     ap.add_argument("--tracer-shape", default="auto",
                     help="auto (autotuned) or <threads>x<CTAs per SM>[-reverse], e.g. 1024x1-reverse")
     ap.add_argument("--no-steady", dest="steady", action="store_false",
