@@ -43,7 +43,8 @@ def available():
 
 
 class RefCudaTracer:
-    """The reference CUDA tracer call (trench_cuda.py:41-138) without record/RF."""
+    """The reference CUDA tracer call (trench_cuda.py:41-138) without record, with the RF
+    in-flight clock (trench_cuda.py:62-72)."""
 
     def __init__(self, vac, device=0):
         import torch
@@ -89,7 +90,7 @@ class RefCudaTracer:
             raise RuntimeError(f"cuLaunchKernel failed ({r})")
         self.launches += 1
 
-    def __call__(self, x, y, vx, vy, qm, spc, Ex, Ey, vac, p, barrier=None):
+    def __call__(self, x, y, vx, vy, qm, spc, Ex, Ey, vac, p, barrier=None, rf=None):
         torch = self.torch
         if vac.shape != self.vac.shape or not np.array_equal(vac, self.vac):
             raise ValueError("geometry changed")
@@ -108,6 +109,15 @@ class RefCudaTracer:
             phi = torch.from_numpy(np.ascontiguousarray(barrier[0], dtype=np.float64)).to(dev)
             wface = torch.from_numpy(np.ascontiguousarray(barrier[1], dtype=np.float64)).to(dev)
         tapered = int(bool(p.trench_taper_deg or (p.mask_t > 0 and p.mask_taper_deg)))
+        d64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+        if rf is None:
+            rf_ex = rf_ey = rf_phi = wave = clocks = self.dummy
+            period, dt_max, n_phase, bound = 1.0, 1.0, 0, np.zeros(2)
+        else:
+            rf_ex, rf_ey, rf_phi, wave = (d64(rf[k]) for k in ("Ex", "Ey", "phi", "wave"))
+            clocks = d64(np.column_stack((np.asarray(rf["initial_time"]) % rf["period"], np.zeros(n))))
+            period, dt_max, n_phase = float(rf["period"]), float(rf["dt_max"]), len(rf["wave"])
+            bound = np.abs(np.asarray(rf["wave"])).max(axis=0)
         host_status = np.full(n, 3, dtype=np.int8)
         dp = lambda t: t.data_ptr()
         for offset in range(0, p.max_steps, 256):               # trench_cuda.py:100-117
@@ -117,12 +127,11 @@ class RefCudaTracer:
                     ("p", dp(phi)), ("p", dp(wface)), ("p", dp(status)), ("p", dp(hits)),
                     ("p", dp(self.dummy)), ("p", dp(self.dummy_int)), ("p", dp(self.dummy)),
                     ("p", dp(self.dummy_int)),
-                    ("p", dp(self.dummy)), ("p", dp(self.dummy)), ("p", dp(self.dummy)), ("p", dp(self.dummy)),
-                    ("p", dp(self.dummy)),
+                    ("p", dp(rf_ex)), ("p", dp(rf_ey)), ("p", dp(rf_phi)), ("p", dp(wave)), ("p", dp(clocks)),
                     ("i", n), ("i", nx), ("i", ny), ("i", min(256, p.max_steps - offset)), ("i", int(offset == 0)),
                     ("i", int(barrier is not None)), ("i", 0), ("i", tapered), ("i", p.max_steps + 1),
-                    ("d", float(p.dx)), ("d", float(p.cfl)), ("i", 0), ("d", 1.0), ("d", 1.0), ("d", 0.0),
-                    ("d", 0.0)]
+                    ("d", float(p.dx)), ("d", float(p.cfl)), ("i", n_phase), ("d", period), ("d", dt_max),
+                    ("d", float(bound[0])), ("d", float(bound[1]))]
             self._launch((n + 127) // 128, args)
             host_status = status.cpu().numpy()                   # synchronises, once per chunk
         host_hits = hits.cpu().numpy()

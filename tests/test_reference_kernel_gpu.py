@@ -95,3 +95,76 @@ def test_speed_against_plain_fp64_gpu_form(cuda_device):
         with open(os.path.join(out, "reference_kernel.json"), "w") as fh:
             json.dump(report, fh, indent=1)
     assert t_f32 < t_ref
+
+
+def rf_of(g):
+    return dict(period=float(g["rf_period"]), dt_max=float(g["rf_dt_max"]), wave=g["rf_wave"], phi=g["rf_phi"],
+                Ex=g["rf_Ex"], Ey=g["rf_Ey"], initial_time=g["rf_initial_time"])
+
+
+def test_reference_kernel_with_rf_clock_reproduces_reference_cpu_and_b200_fp64(cuda_device):
+    """The in-flight RF clock: the reference kernel, the reference CPU tracer (fixture) and the
+    B200 FP64 kernel give the same counts."""
+    from trench_b200.tracer import B200Tracer
+    g = load_golden("trace_rf_taper.npz")
+    args = (g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
+    got = ref_cuda.RefCudaTracer(~g["solid"], cuda_device)(*parts(g), *args, rf=rf_of(g))
+    mine = B200Tracer(~g["solid"], cuda_device, precision="f64")(*parts(g), *args, rf=rf_of(g))
+    for a, b, want in zip(got, mine, (g["cnt_i"], g["cnt_e"], g["escaped"])):
+        np.testing.assert_array_equal(a, want)
+        np.testing.assert_array_equal(b, want)
+    assert got[3] == mine[3] == int(g["lost"])
+
+
+def test_circuit_rf_batch_against_the_reference_kernel(cuda_device):
+    """One batch of the reference's circuit_rf benchmark run (120 x 560 grid, pulsed 5 kV,
+    3000 ions + 3000 electrons at stratified phases): the reference kernel driven like the
+    reference and the B200 FP64 kernel give the same counts; the B200 FP32 kernel agrees on
+    >= 99.9 % of the particles' outcomes and is faster than the reference kernel."""
+    import torch
+    import bench
+    from trench_b200 import geometry, inject
+    from trench_b200.fields import compute_field, setup_fields
+    from trench_b200.tracer import B200Tracer
+    p, circuit, _, _ = bench.rf_cycle_workload()
+    solid, mask, _, _ = geometry.build_geometry(p)
+    f = setup_fields(p, solid, mask, circuit, device=cuda_device)
+    ex, ey = compute_field(f["external"], ~solid, p, f["volts"]["top"])
+    wface = np.where(f["cond"], 1.0, f["eps"] / (1 + f["eps"]))
+    rng = np.random.default_rng(9)
+    prt = inject.inject(p, p.n_per_batch, solid.shape[1], rng, ion_energy=lambda r, k: np.full(k, p.electron_temp_eV / 2))
+    rf = {**f["rf"], "initial_time": np.concatenate([inject.launch_times(rng, p.n_per_batch, f["rf"]["period"])
+                                                     for _ in range(2)])}
+    args = (ex, ey, ~solid, p, (f["external"], wface))
+    ref = ref_cuda.RefCudaTracer(~solid, cuda_device)
+    f64 = B200Tracer(~solid, cuda_device, precision="f64")
+    f32 = B200Tracer(~solid, cuda_device, precision="f32")
+
+    def timed(fn, reps):
+        out, ts = None, []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = fn(*(a.copy() for a in prt), *args, rf=rf)
+            torch.cuda.synchronize()
+            ts.append(time.perf_counter() - t0)
+        return out, min(ts)
+
+    r_ref, t_ref = timed(ref, 2)
+    r_f64, t_f64 = timed(f64, 2)
+    r_f32, t_f32 = timed(f32, 3)
+    for a, b in zip(r_ref[:3], r_f64[:3]):
+        np.testing.assert_array_equal(a, b)
+    assert r_ref[3] == r_f64[3]
+    same = (f32.last["status"] == f64.last["status"]) & (f32.last["hit"] == f64.last["hit"])
+    report = {"workload": "circuit_rf benchmark run, one batch of 6000 particles", "reference_fp64_kernel_s": t_ref,
+              "b200_f64_call_s": t_f64, "b200_f32_call_s": t_f32, "f32_agreement": float(same.mean()),
+              "reference_launches": ref.launches}
+    print(json.dumps(report))
+    out = os.environ.get("TB_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, "reference_kernel_rf.json"), "w") as fh:
+            json.dump(report, fh, indent=1)
+    assert same.mean() >= 0.999
+    assert t_f32 < t_ref

@@ -22,8 +22,22 @@ struct K64 {
     int *err;
 };
 
-// NumPy float remainder for a positive modulus (trench_charging_2d.py:606).
+// NumPy float remainder for a positive modulus (trench_charging_2d.py:606).  A value at
+// most one period outside [0, b) -- every position after one step and every clock -- is
+// wrapped by one exact subtraction (b <= a < 2b: exact by Sterbenz's lemma) or by the same
+// rounded addition NumPy makes for a negative remainder; FP64 fmod, an iterative routine,
+// is left for the rest.  Results are identical to the general form, including +0 for a
+// remainder of zero.
 __device__ __forceinline__ double pymod(double a, double b) {
+    if (a >= 0.0 && a < b) return a == 0.0 ? 0.0 : a;
+    if (a >= b && a < 2.0 * b) {
+        const double m = a - b;
+        return m == 0.0 ? 0.0 : m;
+    }
+    if (a < 0.0 && a >= -b) {
+        const double m = a + b;
+        return m == 0.0 ? 0.0 : m;
+    }
     double m = fmod(a, b);
     if (m != 0.0) {
         if ((m < 0.0) != (b < 0.0)) m += b;
@@ -33,26 +47,31 @@ __device__ __forceinline__ double pymod(double a, double b) {
     return m;
 }
 
-__device__ __forceinline__ long long clipll(long long i, long long n) {
+__device__ __forceinline__ int clipll(int i, int n) {
     return i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
 }
-__device__ __forceinline__ long long pmodll(long long i, long long n) {
-    long long r = i % n;
+// i mod n in [0, n); indices at most one period out are wrapped without a division.
+// Cell indices are 32-bit, as in the reference kernel (grids hold fewer than 2^31 cells).
+__device__ __forceinline__ int pmodll(int i, int n) {
+    if (i >= 0 && i < n) return i;
+    if (i >= n && i < 2 * n) return i - n;
+    if (i < 0 && i >= -n) return i + n;
+    int r = i % n;
     return r < 0 ? r + n : r;
 }
 
 // Vacuum-weighted bilinear field (trench_charging_2d.py:492-509).
 __device__ __forceinline__ void interp(const K64 &k, const double *ex, const double *ey, double x, double y,
                                        double &ox, double &oy) {
-    const long long nx = k.nx, ny = k.ny;
+    const int nx = k.nx, ny = k.ny;
     double fx = x / k.dx - 0.5, fy = y / k.dx - 0.5;
-    long long i0 = (long long)floor(fx), j0 = (long long)floor(fy);
+    int i0 = (int)floor(fx), j0 = (int)floor(fy);
     double tx = fx - (double)i0, ty = fy - (double)j0;
-    long long i1 = pmodll(i0 + 1, nx);
+    int i1 = pmodll(i0 + 1, nx);
     i0 = pmodll(i0, nx);
-    long long j1 = clipll(j0 + 1, ny);
+    int j1 = clipll(j0 + 1, ny);
     j0 = clipll(j0, ny);
-    const long long c[4] = {i0 * ny + j0, i1 * ny + j0, i0 * ny + j1, i1 * ny + j1};
+    const int c[4] = {i0 * ny + j0, i1 * ny + j0, i0 * ny + j1, i1 * ny + j1};
     const double w[4] = {(1.0 - tx) * (1.0 - ty), tx * (1.0 - ty), (1.0 - tx) * ty, tx * ty};
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
@@ -72,22 +91,22 @@ __device__ __forceinline__ void interp(const K64 &k, const double *ex, const dou
 
 // First solid face crossed by a move (trench_charging_2d.py:512-539).
 __device__ __forceinline__ void wall_entry(const K64 &k, double x0, double y0, double sx, double sy,
-                                           long long &cx, long long &cy, long long &vcx, long long &vcy,
+                                           int &cx, int &cy, int &vcx, int &vcy,
                                            bool &face_x) {
-    const long long nx = k.nx, ny = k.ny;
+    const int nx = k.nx, ny = k.ny;
     const double dx = k.dx;
-    long long ix0 = (long long)(x0 / dx);
+    int ix0 = (int)(x0 / dx);
     if (ix0 > nx - 1) ix0 = nx - 1;
-    const long long iy0 = clipll((long long)(y0 / dx), ny);
+    const int iy0 = clipll((int)(y0 / dx), ny);
     const double xu = x0 + sx, yu = y0 + sy;
-    const long long dix = (long long)floor(xu / dx) - ix0;
-    const long long diy = clipll((long long)floor(yu / dx), ny) - iy0;
+    const int dix = (int)floor(xu / dx) - ix0;
+    const int diy = clipll((int)floor(yu / dx), ny) - iy0;
     const double inf = __longlong_as_double(0x7ff0000000000000LL);
     const double fx = dix != 0 ? ((double)(ix0 + (dix > 0)) * dx - x0) / sx : inf;
     const double fy = diy != 0 ? ((double)(iy0 + (diy > 0)) * dx - y0) / sy : inf;
     const bool x_first = fx < fy;
-    const long long ax = x_first ? pmodll(ix0 + dix, nx) : ix0;
-    const long long ay = x_first ? iy0 : iy0 + diy;
+    const int ax = x_first ? pmodll(ix0 + dix, nx) : ix0;
+    const int ay = x_first ? iy0 : iy0 + diy;
     const bool use_last = dix != 0 && diy != 0 && __ldg(k.vac + ax * ny + ay);
     cx = use_last ? pmodll(ix0 + dix, nx) : ax;
     cy = use_last ? iy0 + diy : ay;
@@ -99,8 +118,8 @@ __device__ __forceinline__ void wall_entry(const K64 &k, double x0, double y0, d
 // Periodic linear interpolation of the electrode voltage deltas (trench_rf.py:5-11).
 __device__ __forceinline__ void rf_coeff(const K64 &k, double at, double &vs, double &vm) {
     const double f = pymod(at, k.a.period) / k.a.period * (double)k.a.n_phase;
-    const long long i = pmodll((long long)floor(f), k.a.n_phase);
-    const long long j = pmodll(i + 1, k.a.n_phase);
+    const int i = pmodll((int)floor(f), k.a.n_phase);
+    const int j = pmodll(i + 1, k.a.n_phase);
     const double w = f - floor(f);
     vs = k.a.d_wave[2 * i] * (1.0 - w) + k.a.d_wave[2 * j] * w;
     vm = k.a.d_wave[2 * i + 1] * (1.0 - w) + k.a.d_wave[2 * j + 1] * w;
@@ -110,8 +129,8 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const tb_trace_args &a = k.a;
-    const long long nx = k.nx, ny = k.ny;
-    const long long cells = nx * ny;
+    const int nx = k.nx, ny = k.ny;
+    const int cells = nx * ny;
     const double dx = k.dx, Lx = (double)nx * dx, Ly = (double)ny * dx;
     const bool rf = a.n_phase > 0;
 
@@ -188,16 +207,16 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
         ++my_steps;
 
         const bool escaped = y >= Ly;
-        long long ix = (long long)(x / dx);
+        int ix = (int)(x / dx);
         if (ix > nx - 1) ix = nx - 1;
-        long long iy = clipll((long long)(y / dx), ny);
+        int iy = clipll((int)(y / dx), ny);
         bool hit = !escaped && !__ldg(k.vac + ix * ny + iy);
-        long long cx = 0, cy = 0, vcx = 0, vcy = 0;
+        int cx = 0, cy = 0, vcx = 0, vcy = 0;
         bool face_x = false;
         if (a.tapered && !hit && !escaped) {
-            long long ix0 = (long long)(x0 / dx);
+            int ix0 = (int)(x0 / dx);
             if (ix0 > nx - 1) ix0 = nx - 1;
-            const long long iy0 = clipll((long long)(y0 / dx), ny);
+            const int iy0 = clipll((int)(y0 / dx), ny);
             if (ix != ix0 && iy != iy0) {
                 wall_entry(k, x0, y0, sx, sy, cx, cy, vcx, vcy, face_x);
                 hit = !__ldg(k.vac + cx * ny + cy);
@@ -206,7 +225,7 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
         if (a.d_phi && hit) {
             wall_entry(k, x0, y0, sx, sy, cx, cy, vcx, vcy, face_x);
             const double vn = face_x ? vx : vy;
-            const long long cc = cx * ny + cy, vv = vcx * ny + vcy;
+            const int cc = cx * ny + cy, vv = vcx * ny + vcy;
             double dphi = a.d_wface[cc] * (a.d_phi[cc] - a.d_phi[vv]);
             if (rf) {
                 double vs, vm;
@@ -265,7 +284,7 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
 
         int done = 0;  // 1 absorbed, 2 escaped, 3 budget or step cap reached
         if (hit) {
-            const long long cell = ix * ny + iy;
+            const int cell = ix * ny + iy;
             if (cell < 0 || cell >= cells) {
                 atomicCAS(k.err, TB_DERR_NONE, TB_DERR_BAD_CELL);
             } else {
@@ -330,7 +349,9 @@ int tb_launch_trace_f64(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.queue = ctx->d_queue;
     k.err = ctx->d_err;
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
-    const int threads = 256;
+    // a batch too small to give every SM a 256-thread CTA is spread over more SMs in
+    // 128-thread CTAs (FP64 issue per SM is the limit while the batch is full)
+    const int threads = a->n >= (long long)ctx->num_sms * 256 ? 256 : 128;
     long long want = (a->n + threads - 1) / threads;
     long long cap = (long long)ctx->num_sms * 8;
     int blocks = (int)(want < cap ? want : cap);
