@@ -99,7 +99,8 @@ int tb_set_fields(tb_ctx *ctx, const double *d_ex, const double *d_ey, const dou
  * tb_set_fields (call it again after a tb_set_fields with another vscale), and the
  * waveform as one float4 per table interval.  The basis and waveform are fixed for a
  * case, so one call serves every batch; tb_trace then requires args->d_wave and
- * n_phase to be the ones given here.  Replaces the copies of rf_ex/rf_ey/rf_phi/wave
+ * n_phase to be the ones given here.  A later call with a longer waveform moves the
+ * table: capture CUDA graphs of traces after the last call.  Replaces the copies of rf_ex/rf_ey/rf_phi/wave
  * in CudaTracer.__call__ (trench_cuda.py:63-70). */
 int tb_set_rf_fields(tb_ctx *ctx, const double *d_rf_ex, const double *d_rf_ey, const double *d_rf_phi,
                      const double *d_wface, const double *d_wave, int n_phase, void *stream);
