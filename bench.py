@@ -186,8 +186,10 @@ def run_reference(args, p):
     sample = 1 << 13
     steps = []
     base = None
+    # each timed step is a bounded sample, sized so the whole run takes about three minutes
+    per_step = float(np.clip(150.0 / max(args.steps, 1), 1.0, 8.0))
     for i in range(args.warmup + args.steps):
-        b = cpu_baseline(p, sample, seconds_budget=8.0 if i >= args.warmup else 2.0)
+        b = cpu_baseline(p, sample, seconds_budget=per_step if i >= args.warmup else 1.0)
         if i >= args.warmup:
             steps.append(b)
         base = b
