@@ -1,6 +1,7 @@
 """Steady-state stopping: the check functions against the reference's outputs on
 seeded synthetic histories (trench_charging_2d.py:877-945)."""
 import numpy as np
+import pytest
 
 from conftest import load_golden
 from trench_b200 import steady
@@ -58,3 +59,67 @@ def test_potential_scale_is_the_charging_potential_not_the_rf_bias():
     no_bias = steady.check_steady({"wall": charging}, ["wall"], p, dict(wall=0))
     assert not correct[0]
     np.testing.assert_allclose(correct[2:], no_bias[2:], rtol=1e-12)
+
+
+def _p(**changes):
+    from dataclasses import replace
+    from trench_b200.params import Params
+    return replace(Params(), steady_window=30, **changes)
+
+
+@pytest.mark.parametrize("sign", [-1, 1])
+@pytest.mark.parametrize("age", [10_000, 1_000_000])
+def test_constant_charging_fails_the_drift_check_although_the_means_are_close(sign, age):
+    """A steady current passes the relative block-mean test after a long run but not the drift
+    test (tests/test_steady_charge.py:17-28)."""
+    p = _p()
+    W = p.steady_window
+    q = sign * (age + np.arange(2 * W)) * 1e-12
+    cur, prev = q[-W:].mean(), q[:W].mean()
+    assert abs(cur - prev) < p.steady_charge_rtol * max(abs(cur), abs(prev))
+    check = steady.check_charge_steady({"right": q}, p)
+    assert not check["ok"] and check["kind"] == "drift"
+    np.testing.assert_allclose(check["d"], sign * W * 1e-12, rtol=1e-8)
+    np.testing.assert_allclose(check["rate"], sign * 1e-12 / p.dt_batch, rtol=1e-8)
+
+
+@pytest.mark.parametrize("seed", [3, 17])
+def test_stationary_charge_with_sampling_noise_passes(seed):
+    p = _p()
+    noise = np.random.default_rng(seed).normal(0, 0.01e-12, 2 * p.steady_window)
+    assert steady.check_charge_steady({"left": 20e-12 + noise, "right": -50e-12 - noise}, p)["ok"]
+
+
+def test_a_recent_step_fails_the_block_mean_check():
+    p = _p()
+    q = np.r_[np.full(p.steady_window, 20e-12), np.full(p.steady_window, 21e-12)]
+    check = steady.check_charge_steady({"bottom": q}, p)
+    assert not check["ok"] and check["kind"] == "mean"
+    np.testing.assert_allclose(check["d"], 1e-12)
+
+
+def test_opposite_walls_and_the_absolute_surface_charge_are_checked_separately():
+    p = _p()
+    q = (100 + np.arange(2 * p.steady_window) * 0.05) * 1e-12
+    check = steady.check_charge_steady({"left": q, "right": -q, "surface": q - q}, p)
+    assert not check["ok"] and check["name"] in ("left", "right")
+    g = np.arange(2 * p.steady_window) * 1e-12
+    check = steady.check_charge_steady({"surface": np.zeros_like(g), "surface absolute": g}, p)
+    assert not check["ok"] and check["name"] == "surface absolute"
+
+
+def test_negligible_drift_uses_the_absolute_tolerance():
+    from dataclasses import replace
+    p = _p()
+    q = np.arange(2 * p.steady_window) * (p.steady_charge_atol / (2 * p.steady_window))
+    assert steady.check_charge_steady({"left": q}, p)["ok"]
+    assert steady.check_charge_steady({"left": np.zeros_like(q)}, replace(p, steady_charge_atol=0))["ok"]
+
+
+@pytest.mark.parametrize("changes", [dict(steady_charge_rtol=0), dict(steady_charge_rtol=np.nan),
+                                     dict(steady_charge_atol=-1), dict(steady_charge_atol=np.inf),
+                                     dict(steady_window=4), dict(dt_batch=0)])
+def test_invalid_charge_criterion_is_rejected(changes):
+    from dataclasses import replace
+    with pytest.raises(ValueError):
+        steady.check_charge_steady({"left": np.zeros(60)}, replace(_p(), **changes))
