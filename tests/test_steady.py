@@ -123,3 +123,26 @@ def test_invalid_charge_criterion_is_rejected(changes):
     from dataclasses import replace
     with pytest.raises(ValueError):
         steady.check_charge_steady({"left": np.zeros(60)}, replace(_p(), **changes))
+
+
+@pytest.mark.parametrize("mask_type", ["conductor", "dielectric"])
+def test_charge_monitors_cover_both_walls_height_bands_floor_and_mask(mask_type):
+    """tests/test_steady_charge.py:77-99: the monitor regions of the charge check."""
+    from dataclasses import replace
+    from trench_b200 import geometry
+    from trench_b200.params import Params
+    p = replace(Params(), nx=20, trench_w=6, trench_d=12, floor_t=4, mask_t=4, n_vac=8, mask_type=mask_type)
+    solid, mask, i0, i1 = geometry.build_geometry(p)
+    regions = steady.charge_monitors(solid, mask, i0, i1, p)
+    rho = np.zeros(solid.shape)
+    rho[i0 - 1, p.floor_t + 1] = 3 / p.dx ** 2
+    rho[i0 - 1, p.floor_t + p.trench_d - 1] = -3 / p.dx ** 2
+    rho[i1, p.floor_t + 1] = 2 / p.dx ** 2
+    rho[i0 + 1, p.floor_t - 1] = 5 / p.dx ** 2
+    rho.flat[np.flatnonzero(mask & geometry.surface_cells(solid))[0]] = 7 / p.dx ** 2
+    q = {k: rho.ravel()[idx].sum() * p.dx ** 2 for k, idx in regions.items()}
+    absolute = np.abs(rho.ravel()[regions["surface"]]).sum() * p.dx ** 2
+    np.testing.assert_allclose([q["left"], q["left band 1"], q["left band 3"], q["right"], q["bottom"], q["mask"]],
+                               [0, 3, -3, 2, 5, 7], atol=1e-12)
+    np.testing.assert_allclose(q["surface"], 7 if mask_type == "conductor" else 14)
+    np.testing.assert_allclose(absolute, 13 if mask_type == "conductor" else 20)
