@@ -100,3 +100,28 @@ def test_full_cycle_probe_uses_identical_phases_and_preserves_charge(cuda_device
     np.testing.assert_array_equal(res["rho_raw"], before)
     for label in ("charged", "uncharged"):
         assert d[label]["hits"].sum() + d[label]["escaped"] + d[label]["lost"] == p.probe_ions
+
+
+def test_tapered_monitors_partition_the_walls_and_catch_every_vertical_ion(cuda_device):
+    """tests/test_taper.py:92-110: on a tapered trench the monitors include the horizontal steps,
+    the height bands partition each sidewall, and every ion of an uncharged vertical beam lands
+    on a sidewall, the floor or the mask (40 / 40 / 48 of 224 on the sidewalls and floor)."""
+    from trench_b200 import steady
+    from trench_b200.probe import probe_vertical_ions
+    tr, ma = np.degrees(np.arctan(0.25)), np.degrees(np.arctan(0.5))
+    p = replace(Params(), nx=40, trench_w=16, trench_d=20, floor_t=4, mask_t=12, n_vac=10, trench_taper_deg=tr,
+                mask_taper_deg=ma, bias="dc", sigma_s=0, n_batches=3, n_per_batch=256, max_steps=800,
+                probe_ions=224, probe_trajectories=12)
+    solid, mask, i0, i1 = geometry.build_geometry(p)
+    regions = steady.charge_monitors(solid, mask, i0, i1, p)
+    left = np.unravel_index(regions["left"], solid.shape)
+    assert len(np.unique(left[0])) > 1
+    res = dict(params=asdict(p), solid=solid, mask=mask, rho_raw=np.zeros(solid.shape), t_conv=1e-3, stopped=False)
+    hits = probe_vertical_ions(res, log=None, device=cuda_device)["uncharged"]["hits"]
+    flat = hits.ravel()
+    assert flat[regions["left"]].sum() + flat[regions["right"]].sum() + flat[regions["bottom"]].sum() \
+        + hits[mask].sum() == p.probe_ions
+    for side in ("left", "right"):
+        bands = [regions[f"{side} band {b}"] for b in (1, 2, 3)]
+        np.testing.assert_array_equal(np.sort(np.concatenate(bands)), regions[side])
+    assert (flat[regions["left"]].sum(), flat[regions["right"]].sum(), flat[regions["bottom"]].sum()) == (40, 40, 48)
