@@ -73,3 +73,15 @@ def test_tracer_without_gpu_fails_loudly():
     from trench_b200.tracer import B200Tracer
     with pytest.raises(RuntimeError):
         B200Tracer(np.ones((4, 5), bool))
+
+
+def test_entry_points_reject_a_missing_context(lib):
+    """Every call taking a context returns TB_ERR_ARG for a null one, without touching a device."""
+    null = None
+    assert lib.tb_set_rf_fields(null, null, null, null, null, null, 0, null) == _capi.TB_ERR_ARG
+    assert lib.tb_set_tuning(null, 1024, 1) == _capi.TB_ERR_ARG
+    assert lib.tb_set_claim_order(null, 0) == _capi.TB_ERR_ARG
+    assert lib.tb_trace(null, null, 1, null) == _capi.TB_ERR_ARG
+    assert lib.tb_check(null, null) == _capi.TB_ERR_ARG
+    assert lib.tb_inject(null, null, null) == _capi.TB_ERR_ARG
+    assert lib.tb_pack_trace(null, 1, null) == _capi.TB_ERR_ARG
