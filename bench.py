@@ -391,6 +391,34 @@ def run_b200(args, p):
     return 0
 
 
+def sweep_cpu_baseline(ps, seps, seconds_budget=15.0, per_species=1 << 12):
+    """The oracle (FP64 C tracer on all host threads + the FP64 batch update) on the sweep's
+    cases in turn, each with a bounded sample of its own distributions: particles/s."""
+    from oracle import oracle_fields as OF
+    from oracle import oracle_trace as OT
+    from trench_b200 import geometry, inject
+    threads = OT.default_threads()
+    rng = np.random.default_rng(12)
+    done, t_total, cases = 0, 0.0, 0
+    for p, sep in zip(ps[:16], seps[:16]):
+        if t_total >= seconds_budget:
+            break
+        q = replace(p, n_per_batch=per_species)
+        solid, mask, _, _ = geometry.build_geometry(q)
+        st = OF.BatchState(q, solid, mask)
+        energy = inject.mixture_energy([(0.5, "normal", 40.0, 6.0), (0.5, "normal", 40.0 + sep, 6.0)])
+        sampler = inject.energy_angle_sampler(q, energy, inject.half_gaussian_angle(3.0))
+        parts = inject.inject(q, q.n_per_batch, solid.shape[1], rng, ion_velocity=sampler)
+        t0 = time.perf_counter()
+        st.step(*OT.trace(*parts, st.Ex, st.Ey, ~solid, q, st.barrier(), threads=threads))
+        t_total += time.perf_counter() - t0
+        done += 2 * per_species
+        cases += 1
+    return {"value": done / t_total, "unit": "particles/s", "cores": threads, "kind": "port",
+            "sample": f"one batch of {2 * per_species} particles on each of the first {cases} sweep cases "
+                      f"(their own geometry and distributions), trace + batch update, {t_total:.1f} s"}
+
+
 def run_sweep(args):
     """Batched sweep: 64 uneven cases advanced together, one persistent tracer launch per
     batch (configuration 3); reported as particles/s over all cases."""
@@ -440,7 +468,7 @@ def run_sweep(args):
                                    "bimodal IED separation 30-150 eV", "cases": len(ps),
                        "particles_per_batch": total, "setup_s": setup_s},
             "batches_per_s": 1000.0 / float(np.mean(ms)), "particle_steps_per_batch": float(steps_per_batch),
-            "clocks": clk,
+            "clocks": clk, "cpu_baseline": sweep_cpu_baseline(ps, seps, seconds_budget=args.cpu_seconds),
             # per step: the pack's reset and tracer launches, then per case the fused charge update
             # (surface cells <= 1024 in every sweep case), Green's GEMV and field
             "gpu_launches": (2 + 3 * len(ps)) * args.steps}
