@@ -134,8 +134,14 @@ class ChargingCase:
                 mask_rhs = np.zeros((nx, ny))
             rhs = boundary_rhs(p, eps, volts)
             self.boundary_rhs = rhs
-            self.external = (solver.solve((rhs + mask_rhs).ravel()) + phi_cond.ravel()).reshape(nx, ny)
             self.floating = bool(cond.any() and not driven)
+            # the external potential's and the floating conductor's solves run in the block of the
+            # surface Green's solves below (independent right-hand sides of the same operator)
+            extra = [(rhs + mask_rhs).ravel()]
+            if self.floating:
+                g_rhs = np.zeros(self.n)
+                g_rhs[np.flatnonzero(cond)[0]] = -1.0 / (p.dx ** 2 * EPS0)
+                extra.append(g_rhs)
             self.driven = driven
             wface = np.where(cond, 1.0, eps / (1.0 + eps))
             self.wface = wface
@@ -157,7 +163,8 @@ class ChargingCase:
                 b = torch.where(self.solver.cond_t[None, :], torch.zeros_like(b), b)
                 self.tuning["poisson"] = {str(k_): v for k_, v in self.solver.autotune(b).items()}
             self.tuning["poisson_schedule"] = self.solver.schedule_used
-            self._build_green(rows, green)
+            sol = self._build_green(rows, green, np.array(extra))
+            self.external = (sol[0] + phi_cond.ravel()).reshape(nx, ny)
             if solver.max_rhs * self.n * (FieldSolver.BYTES_PER_RHS_CELL // 2) > FieldSolver.KEEP_BYTES:
                 solver.resize(max_rhs)
             # leakage (trench_charging_2d.py:768-803)
@@ -181,9 +188,7 @@ class ChargingCase:
             self.g_s = None
             self.C_cond, self.c_slot = 0.0, -1
             if self.floating:
-                b = np.zeros(self.n)
-                b[np.flatnonzero(cond)[0]] = -1.0 / (p.dx ** 2 * EPS0)
-                g = solver.solve(b)
+                g = sol[1]
                 self.g_cond = g.reshape(nx, ny)
                 self.C_cond = 1.0 / g[np.flatnonzero(cond)[0]]
                 c_cell = np.flatnonzero(geometry.surface_cells(solid) & cond)[0]
@@ -258,25 +263,40 @@ class ChargingCase:
                     _ptr(self.t_rf["wave"]), len(self.rf["wave"]), self._stream()))
 
     # ---- setup helpers -----------------------------------------------------------
-    def _build_green(self, rows, green):
-        """G[r, j] = potential at rows[r] per unit charge density on surface cell j."""
+    def _build_green(self, rows, green, extra=None):
+        """G[r, j] = potential at rows[r] per unit charge density on surface cell j.  `extra`:
+        optional (k, n) right-hand sides b of A phi = b solved in the same blocks, ahead of the
+        Green's columns; returns their solutions (k, n) on the host."""
         p, dev, S, m = self.p, self.dev, self.S, self.m
         dtype = torch.float32 if green == "f32" else torch.float64
         G = torch.empty((len(rows), m), dtype=dtype, device=dev)
         P = torch.empty((m, m), dtype=torch.float64, device=dev)
         t_rows = torch.from_numpy(rows).to(dev)
         t_S = torch.from_numpy(S).to(dev)
+        k_extra = 0 if extra is None else len(extra)
+        t_extra = torch.from_numpy(np.ascontiguousarray(extra, dtype=np.float64)).to(dev) if k_extra else None
+        solved = []
         chunk = self.solver.max_rhs
-        for s in range(0, m, chunk):
-            e = min(m, s + chunk)
+        total = k_extra + m
+        for s in range(0, total, chunk):
+            e = min(total, s + chunk)
             b = torch.zeros((e - s, self.n), dtype=torch.float64, device=dev)
-            b[torch.arange(e - s, device=dev), t_S[s:e]] = -1.0 / EPS0
+            n_ex = max(0, min(e, k_extra) - s)                 # extra rows in this block
+            if n_ex:
+                b[:n_ex] = t_extra[s:s + n_ex]
+            g0, g1 = s + n_ex - k_extra, e - k_extra            # Green's columns in this block
+            if g1 > g0:
+                b[n_ex + torch.arange(g1 - g0, device=dev), t_S[g0:g1]] = -1.0 / EPS0
             x = self.solver.solve_rows(b)
-            G[:, s:e] = x[:, t_rows].T.to(dtype)
-            P[:, s:e] = x[:, t_S].T / p.dx ** 2   # per unit charge (1 C/m) on a dx^2 cell
+            if n_ex:
+                solved.append(x[:n_ex].cpu().numpy())
+            if g1 > g0:
+                G[:, g0:g1] = x[n_ex:, t_rows].T.to(dtype)
+                P[:, g0:g1] = x[n_ex:, t_S].T / p.dx ** 2   # per unit charge (1 C/m) on a dx^2 cell
         self.G = G.contiguous()
         self.P = P
         self.green = green
+        return np.concatenate(solved) if solved else None
 
     def _build_rf(self, circuit, solver, eps, cond, vac):
         """Unit-voltage basis of the electrodes and the period-resolved voltage deltas
