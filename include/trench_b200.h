@@ -128,7 +128,10 @@ int tb_set_claim_order(tb_ctx *ctx, int reverse);
 
 /* Synchronise `stream`, then read and clear the context's device-side check flag:
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the
- * grid, a bulk copy that did not complete in its bounded wait). */
+ * grid, a bulk copy that did not complete in its bounded wait).  After
+ * TB_ERR_KERNEL the batch's counts, totals, status and step counts are partial (a
+ * CTA whose field copy timed out returned without tracing its particles): discard
+ * them and trace the batch again. */
 int tb_check(tb_ctx *ctx, void *stream);
 
 /* ---- Poisson: multigrid-preconditioned CG ------------------------------------
@@ -265,7 +268,8 @@ int tb_pack_destroy(tb_pack *pack);
 const char *tb_pack_last_error(const tb_pack *pack);
 int tb_pack_set_args(tb_pack *pack, const tb_trace_args *args);
 int tb_pack_trace(tb_pack *pack, int reset, void *stream);
-/* Synchronise `stream`, then read and clear the pack's device check flag. */
+/* Synchronise `stream`, then read and clear the pack's device check flag; after
+ * TB_ERR_KERNEL the batch's results are partial, as for tb_check. */
 int tb_pack_check(tb_pack *pack, void *stream);
 
 /* ---- No-allocation FP32 tracer ---------------------------------------------------
@@ -279,9 +283,13 @@ int tb_pack_check(tb_pack *pack, void *stream);
  * passes the device vacuum mask d_vac (nx*ny bytes, 1 = vacuum), the FP64 fields
  * in args->d_ex/d_ey (and d_phi/d_wface for the barrier model) and every input and
  * output array.  Grids above TB_NOALLOC_MAX_CELLS cells are rejected (TB_ERR_ARG).
- * args->d_totals[6] receives the device check flag (0 = every bound held).  The
- * first call on a device looks up the array's device address and configures the
- * kernel; make that first call before any stream capture.  All calls share the
+ * args->d_totals[6] receives the device check flag (0 = every bound held; a raised
+ * flag means the batch's results are partial and must be traced again, as after
+ * tb_check's TB_ERR_KERNEL); with n = 0 it is set to 0.  Every call looks up the
+ * array's device address and sets the kernel's shared-memory attribute (host-side
+ * calls that allocate nothing), so a call after a device reset finds the reloaded
+ * module; the first call on a device also loads the module, so make it before any
+ * stream capture.  All calls share the
  * one array, so calls that overlap on the GPU (other streams, other host threads)
  * race: serialise them.  Errors are read with tb_last_error(NULL). */
 #define TB_NOALLOC_MAX_CELLS 65536

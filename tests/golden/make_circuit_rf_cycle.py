@@ -1,7 +1,8 @@
 """Generates circuit_rf_cycle.npz: the RF circuit waveform of the reference's own
 circuit_rf benchmark run, computed by the reference's circuit model here.
 
-    python tests/golden/make_circuit_rf_cycle.py [/path/to/reference]
+    python tests/golden/make_circuit_rf_cycle.py /path/to/reference
+    (or TRENCH01_REFERENCE=/path/to/reference python tests/golden/make_circuit_rf_cycle.py)
 
 The run is the one documented in the reference's docs/rf_cycle_validation.json
 (3000 batches of 3000 ions + 3000 electrons on a 120 x 560 grid, pulsed 5 kV
@@ -20,7 +21,7 @@ from pathlib import Path
 import numpy as np
 
 sys.path.insert(0, str(Path(__file__).resolve().parent))
-from make_golden import import_reference, save  # noqa: E402
+from make_golden import import_reference, reference_dir, save  # noqa: E402
 
 
 def main(ref):
@@ -35,4 +36,4 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir(sys.argv))

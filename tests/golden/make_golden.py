@@ -1,6 +1,7 @@
 """Generates the golden fixtures in this folder by running the reference here.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py /path/to/reference
+    (or TRENCH01_REFERENCE=/path/to/reference python tests/golden/make_golden.py)
 
 The reference (a Python package) is imported from its source tree with a stub
 ``matplotlib`` (only ``use`` and an empty ``pyplot`` are needed on the compute
@@ -31,6 +32,15 @@ from pathlib import Path
 import numpy as np
 
 OUT = Path(__file__).resolve().parent
+
+
+def reference_dir(argv):
+    """The reference's source tree: the first argument, else $TRENCH01_REFERENCE."""
+    import os
+    ref = argv[1] if len(argv) > 1 else os.environ.get("TRENCH01_REFERENCE")
+    if not ref:
+        raise SystemExit("name the reference's source tree: make_golden.py PATH or TRENCH01_REFERENCE=PATH")
+    return ref
 
 
 def import_reference(path):
@@ -350,4 +360,4 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(reference_dir(sys.argv))

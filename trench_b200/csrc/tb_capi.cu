@@ -143,7 +143,8 @@ static int check_device_flag(tb_ctx *ctx, cudaStream_t s) {
     TB_CUDA(ctx, cudaStreamSynchronize(s));
     if (flag != TB_DERR_NONE) {
         TB_CUDA(ctx, cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
-        return tb_fail(ctx, TB_ERR_KERNEL, "kernel check failed (code %d: %s)", flag,
+        return tb_fail(ctx, TB_ERR_KERNEL, "kernel check failed (code %d: %s); the batch's results are partial, "
+                       "trace it again", flag,
                        flag == TB_DERR_BULK_TIMEOUT   ? "bulk copy wait gave up"
                        : flag == TB_DERR_BAD_CELL   ? "deposit cell out of range"
                                                     : "absorbed particle outside the surface cells");

@@ -10,7 +10,8 @@
 
 // Device-side error codes written to tb_ctx::d_err (first error wins).
 #define TB_DERR_NONE 0
-#define TB_DERR_BULK_TIMEOUT 1   // bounded wait on a bulk-copy barrier gave up
+#define TB_DERR_BULK_TIMEOUT 1   // bounded wait on a bulk-copy barrier gave up: the CTA returned
+                                 // untraced, so the batch's outputs are partial
 #define TB_DERR_BAD_CELL 2       // a deposit cell fell outside the grid
 #define TB_DERR_OFF_SURFACE 3    // an absorbed particle was counted outside the surface cells
 

@@ -858,15 +858,6 @@ constexpr size_t NOALLOC_BYTES = NOALLOC_FIELD_BYTES + NOALLOC_BARRIER_BYTES + N
 // not a device address.  The per-device address comes from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-struct NoallocDevice {
-    unsigned char *base = nullptr;  // device address of g_noalloc_scratch on this device
-    int num_sms = 0;
-    int max_smem = 0;
-    int smem_attr_bytes = 0;
-};
-NoallocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
-
 }  // namespace
 
 extern "C" int tb_trace_f32_noalloc(int nx, int ny, double dx, const uint8_t *d_vac, const tb_trace_args *a,
@@ -887,39 +878,41 @@ extern "C" int tb_trace_f32_noalloc(int nx, int ny, double dx, const uint8_t *d_
         return tb_fail(nullptr, TB_ERR_ARG, "tb_trace_f32_noalloc: RF clock and record are not supported");
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    if (e != cudaSuccess || dev < 0)
         return tb_fail(nullptr, TB_ERR_DEVICE, "tb_trace_f32_noalloc: no usable current device");
-    NoallocDevice &d = g_noalloc_dev[dev];
+    cudaStream_t s = (cudaStream_t)stream;
+    if (a->n == 0) {
+        // nothing to trace; the check-flag slot still reports this call
+        if (a->d_totals) {
+            e = cudaMemsetAsync(a->d_totals + 6, 0, sizeof(int64_t), s);
+            if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaMemsetAsync(totals[6])");
+        }
+        return TB_OK;
+    }
+    // The array's device address and the kernels' shared-memory attribute are looked up
+    // and set on every call (host-side calls that allocate nothing), so a call after a
+    // device reset, which reloads the module, uses the new address and attribute.
+    void *ptr = nullptr;
+    e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    int num_sms = 0, max_smem = 0;
+    e = cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaDeviceGetAttribute");
     tb_ctx tmp;  // a view of the static scratch; owns nothing and is never released
     tmp.device = dev;
-    if (!d.base) {
-        // set-up, once per device with that device current
-        void *ptr = nullptr;
-        e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaGetSymbolAddress(g_noalloc_scratch)");
-        cudaDeviceProp prop;
-        e = cudaGetDeviceProperties(&prop, dev);
-        if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaGetDeviceProperties");
-        tmp.max_smem = (int)prop.sharedMemPerBlockOptin;
-        if (tb_configure_trace_f32(&tmp) != TB_OK) return tb_fail(nullptr, TB_ERR_CUDA, "%s", tmp.err);
-        d.num_sms = prop.multiProcessorCount;
-        d.max_smem = tmp.max_smem;
-        d.smem_attr_bytes = tmp.smem_attr_bytes;
-        d.base = static_cast<unsigned char *>(ptr);
-    }
+    tmp.max_smem = max_smem;
+    if (tb_configure_trace_f32(&tmp) != TB_OK) return tb_fail(nullptr, TB_ERR_CUDA, "%s", tmp.err);
+    unsigned char *base = static_cast<unsigned char *>(ptr);
     tmp.nx = nx;
     tmp.ny = ny;
     tmp.dx = dx;
-    tmp.num_sms = d.num_sms;
-    tmp.max_smem = d.max_smem;
-    tmp.smem_attr_bytes = d.smem_attr_bytes;
+    tmp.num_sms = num_sms;
     tmp.d_vac = const_cast<uint8_t *>(d_vac);
-    tmp.d_field = reinterpret_cast<tb_fcell *>(d.base);
-    tmp.d_barrier = reinterpret_cast<float4 *>(d.base + NOALLOC_FIELD_BYTES);
-    tmp.d_queue = reinterpret_cast<unsigned long long *>(d.base + NOALLOC_FIELD_BYTES + NOALLOC_BARRIER_BYTES);
+    tmp.d_field = reinterpret_cast<tb_fcell *>(base);
+    tmp.d_barrier = reinterpret_cast<float4 *>(base + NOALLOC_FIELD_BYTES);
+    tmp.d_queue = reinterpret_cast<unsigned long long *>(base + NOALLOC_FIELD_BYTES + NOALLOC_BARRIER_BYTES);
     tmp.d_err = reinterpret_cast<int *>(tmp.d_queue + 8);
-    cudaStream_t s = (cudaStream_t)stream;
-    if (a->n == 0) return TB_OK;
     // the array keeps the previous call's contents: clear the counters that must start at zero
     e = cudaMemsetAsync(tmp.d_queue, 0, NOALLOC_COUNTER_BYTES, s);
     if (e != cudaSuccess) return tb_cuda_check(nullptr, e, "cudaMemsetAsync(scratch counters)");

@@ -1,19 +1,22 @@
 """Steady-state stopping of the charging loop (``until_steady``).
 
-Restates the reference's stopping rule (trench_charging_2d.py:1216-1229, 1302-1320):
-every ``steady_window`` (W) batches, once 2 W batches of history exist, the mean of
-each potential probe over the last W batches is compared with the W before it, and
-so is every charge monitor together with its net drift; after ``steady_hold``
-consecutive passes the run has converged.
+The stopping rule is the reference's (trench_charging_2d.py:846-947, 1302-1320):
+every ``steady_window`` (W) batches, once two windows of history exist, the last
+window of every potential probe is compared with the window before it, and so is
+every charge monitor together with its net drift over a window; after
+``steady_hold`` consecutive passes the run has converged.  A window's mean is
+compared through a standard error that (1) removes the window's linear trend and
+(2) shrinks the sample size by the lag-1 autocorrelation of what is left (an AR(1)
+effective size n (1 - r1) / (1 + r1), r1 clipped to [0, 0.95]).
 
-  charge_monitors       trench_charging_2d.py:850-868  (cells summed per monitor)
-  mean_and_se           trench_charging_2d.py:877-890  (trend-removed, AR(1)-corrected)
-  check_steady          trench_charging_2d.py:893-914
-  check_charge_steady   trench_charging_2d.py:917-945
-  history_start         trench_charging_2d.py:1034-1041
+Here every check runs over all probes (or monitors) at once: the histories are
+stacked into one (series, samples) array and the window statistics are closed-form
+row reductions -- the trend is the least-squares line about the window's centre
+time, the autocorrelation the Pearson coefficient of the residual against itself one
+batch later.
 
-The monitors themselves are summed on the GPU every batch (tb_step_monitors); the
-checks run on the host every W batches over the history read back once.
+The monitors are summed on the GPU every batch (tb_step_monitors); the checks run
+on the host every W batches over the history read back once.
 """
 import numpy as np
 
@@ -21,105 +24,118 @@ from . import geometry
 
 
 def charge_monitors(solid, mask, i0, i1, p):
-    """Cells of each charge monitor: left / right inner sidewall, bottom, the exposed
-    dielectric surface, three depth bands per sidewall and the mask (flat indices)."""
+    """Flat cell indices of each charge monitor (trench_charging_2d.py:850-868): the
+    left and right inner sidewalls of the dielectric (split at the interface opening's
+    centre), the cells under the trench floor's opening, the exposed dielectric
+    surface, each sidewall in three height bands, and the mask."""
+    nx, ny = solid.shape
+    col, row = np.indices(solid.shape)
+    in_trench_rows = (row >= p.floor_t) & (row < p.floor_t + p.trench_d)
+    inner_wall = geometry.inner_surface_cells(solid, p) & in_trench_rows
+    left_half = col + 0.5 < (i0 + i1) / 2
+    lo, hi = geometry.opening_span(solid, p.floor_t)
+    floor = np.zeros_like(solid)
+    floor[lo:hi, p.floor_t - 1] = True
     exposed = geometry.surface_cells(solid)
-    dielectric = exposed & ~(mask if p.mask_type == "conductor" else np.zeros_like(mask))
-    ix, iy = np.indices(solid.shape)
-    wall = (iy >= p.floor_t) & (iy < p.floor_t + p.trench_d)
-    inner = geometry.inner_surface_cells(solid, p)
-    center = (i0 + i1) / 2
-    b0, b1 = geometry.opening_span(solid, p.floor_t)
-    regions = dict(left=(ix + 0.5 < center) & wall & inner,
-                   right=(ix + 0.5 >= center) & wall & inner,
-                   bottom=(ix >= b0) & (ix < b1) & (iy == p.floor_t - 1), surface=dielectric)
-    for side in ("left", "right"):
-        for band, cells in enumerate(np.array_split(np.arange(p.floor_t, p.floor_t + p.trench_d), 3)):
-            if len(cells):
-                regions[f"{side} band {band + 1}"] = regions[side] & np.isin(iy, cells)
+    if p.mask_type == "conductor":
+        exposed = exposed & ~mask
+    sides = {"left": inner_wall & left_half, "right": inner_wall & ~left_half}
+    regions = {**sides, "bottom": floor, "surface": exposed}
+    # three bands of trench rows, the first (lowest) bands one row longer when the depth
+    # does not divide by three
+    bands = np.array_split(np.arange(p.floor_t, p.floor_t + p.trench_d), 3)
+    for side, cells in sides.items():
+        for k, band in enumerate(bands, start=1):
+            if band.size:
+                regions[f"{side} band {k}"] = cells & (row >= band[0]) & (row <= band[-1])
     if mask.any():
         regions["mask"] = mask
-    return {key: np.flatnonzero(region) for key, region in regions.items()}
+    return {name: np.flatnonzero(r) for name, r in regions.items()}
+
+
+def _window_stats(X):
+    """Mean and trend/autocorrelation-corrected standard error of each row of X
+    (series, samples)."""
+    X = np.atleast_2d(np.asarray(X, dtype=float))
+    n = X.shape[1]
+    tc = np.arange(n) - 0.5 * (n - 1)          # sample times about the window centre
+    mean = X.mean(axis=1)
+    slope = (X - mean[:, None]) @ tc / (tc @ tc)
+    resid = X - mean[:, None] - slope[:, None] * tc
+    resid_c = resid - resid.mean(axis=1, keepdims=True)
+    var = (resid_c ** 2).sum(axis=1) / (n - 2)
+    a, b = resid[:, :-1], resid[:, 1:]
+    a = a - a.mean(axis=1, keepdims=True)
+    b = b - b.mean(axis=1, keepdims=True)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        r1 = (a * b).sum(axis=1) / np.sqrt((a * a).sum(axis=1) * (b * b).sum(axis=1))
+    r1 = np.where((var > 0) & np.isfinite(r1), np.clip(r1, 0.0, 0.95), 0.0)
+    n_eff = np.maximum(n * (1 - r1) / (1 + r1), 1.0)
+    return mean, np.sqrt(var / n_eff)
 
 
 def mean_and_se(x):
-    """Mean of a block and its standard error: the variance of the residual after a
-    linear fit, with the effective sample size n (1 - r1) / (1 + r1) of the residual's
-    lag-1 autocorrelation r1 (clipped to [0, 0.95])."""
-    x = np.asarray(x, dtype=float)
-    n = x.size
-    t = np.arange(n)
-    resid = x - np.polyval(np.polyfit(t, x, 1), t)
-    var = resid.var(ddof=2)
-    r1 = 0.0
-    if var > 0:
-        r1 = np.corrcoef(resid[:-1], resid[1:])[0, 1]
-        r1 = float(np.clip(r1, 0.0, 0.95)) if np.isfinite(r1) else 0.0
-    n_eff = max(n * (1 - r1) / (1 + r1), 1.0)
-    return x.mean(), np.sqrt(var / n_eff)
+    """(mean, standard error) of one window (trench_charging_2d.py:877-890)."""
+    m, se = _window_stats(x)
+    return float(m[0]), float(se[0])
 
 
 def check_steady(hist, probes, p, reference=None):
-    """Probe potentials: |mean of the last W - mean of the W before| <= max(rtol x the
-    largest probe potential (relative to `reference`), 3 x the combined standard error)
-    for every probe.  Returns (ok, worst probe, its difference, its tolerance)."""
+    """Probe potentials (trench_charging_2d.py:893-914): |last window mean - previous
+    window mean| <= max(steady_rtol x the largest last-window potential (measured from
+    `reference` when given, at least 1 V), 3 standard errors of the difference) for every
+    probe.  Returns (ok, the probe furthest from passing, its difference, its tolerance)."""
     W = p.steady_window
-    stats = {k: (mean_and_se(np.asarray(hist[k][-W:])), mean_and_se(np.asarray(hist[k][-2 * W:-W])))
-             for k in probes}
-    scale = max(1.0, max(abs(c[0] - (reference[k] if reference is not None else 0.0))
-                         for k, (c, _) in stats.items()))
-    ok, worst = True, (None, 0.0, 1.0, -1.0)
-    for k, ((m_c, se_c), (m_p, se_p)) in stats.items():
-        d = m_c - m_p
-        tol = max(p.steady_rtol * scale, 3.0 * np.hypot(se_c, se_p))
-        ok &= abs(d) <= tol
-        if abs(d) / tol > worst[3]:
-            worst = (k, d, tol, abs(d) / tol)
-    return ok, worst[0], worst[1], worst[2]
+    names = list(probes)
+    H = np.array([np.asarray(hist[k], dtype=float)[-2 * W:] for k in names])
+    m_new, se_new = _window_stats(H[:, W:])
+    m_old, se_old = _window_stats(H[:, :W])
+    base = np.array([reference[k] for k in names]) if reference is not None else 0.0
+    scale = max(1.0, float(np.max(np.abs(m_new - base))))
+    d = m_new - m_old
+    tol = np.maximum(p.steady_rtol * scale, 3.0 * np.hypot(se_new, se_old))
+    worst = int(np.argmax(np.abs(d) / tol))
+    return bool(np.all(np.abs(d) <= tol)), names[worst], float(d[worst]), float(tol[worst])
 
 
 def check_charge_steady(charge_hist, p):
-    """Charge monitors: the difference of the block means (tolerance max(atol, rtol x
-    charge, 3 standard errors)) and the net drift over a block from the per-batch
-    changes (tolerance max(atol, 3 standard errors)).  Returns the worst check as a
-    dict (name, kind, d, tol, ratio, rate, unit) with `ok` for all of them."""
+    """Charge monitors (trench_charging_2d.py:917-945), two tests per monitor over the
+    last two windows: the window means (tolerance max(atol, rtol x the larger |mean|,
+    3 standard errors)) and the net drift of one window from the batch-to-batch
+    changes (tolerance max(atol, 3 standard errors); a steadily charging surface fails
+    it however large its charge).  Returns the test furthest from passing as a dict
+    (name, kind, d, tol, ratio, rate in C/m/s, unit) with ``ok`` for all of them."""
     W = p.steady_window
-    if (not np.isfinite(p.steady_charge_rtol) or p.steady_charge_rtol <= 0
-            or not np.isfinite(p.steady_charge_atol) or p.steady_charge_atol < 0
-            or W < 5 or not np.isfinite(p.dt_batch) or p.dt_batch <= 0):
-        raise ValueError("the charge tolerances and batch time must be finite and positive (atol >= 0), "
-                         "and the window at least 5")
-    if not charge_hist or any(len(q) < 2 * W for q in charge_hist.values()):
-        raise ValueError("the charge check needs two windows of history")
-    ok, worst = True, None
-    for key, values in charge_hist.items():
-        q = np.asarray(values[-2 * W:], dtype=float)
-        if q.ndim != 1 or not np.isfinite(q).all():
-            raise ValueError("the charge history must be finite")
-        cur, se_cur = mean_and_se(q[-W:])
-        prev, se_prev = mean_and_se(q[:W])
-        difference = float(cur - prev)
-        mean_tol = max(p.steady_charge_atol, p.steady_charge_rtol * max(abs(cur), abs(prev)),
-                       3 * np.hypot(se_cur, se_prev))
-        current, se_current = mean_and_se(np.diff(q))
-        drift = float(current * W)
-        drift_tol = max(p.steady_charge_atol, float(3 * se_current * W))
-        for kind, d, tol in (("mean", difference, mean_tol), ("drift", drift, drift_tol)):
-            passed = abs(d) <= tol
-            ratio = abs(d) / tol if tol > 0 else (0.0 if d == 0 else np.inf)
-            ok &= passed
-            if worst is None or ratio > worst["ratio"]:
-                worst = dict(name=key, kind=kind, d=d, tol=float(tol), ratio=float(ratio),
-                             rate=float(current / p.dt_batch), unit="C/m")
-    return {**worst, "ok": bool(ok)}
+    rtol, atol, dt = p.steady_charge_rtol, p.steady_charge_atol, p.dt_batch
+    if not (np.isfinite(rtol) and rtol > 0 and np.isfinite(atol) and atol >= 0 and W >= 5
+            and np.isfinite(dt) and dt > 0):
+        raise ValueError("the charge check needs rtol > 0, atol >= 0 (finite), dt_batch > 0 and a window of "
+                         "at least 5 batches")
+    names = list(charge_hist)
+    if not names or min(len(v) for v in charge_hist.values()) < 2 * W:
+        raise ValueError("the charge check needs two windows of history for every monitor")
+    Q = np.array([np.asarray(charge_hist[k], dtype=float)[-2 * W:] for k in names])
+    if Q.ndim != 2 or not np.isfinite(Q).all():
+        raise ValueError("the charge history holds non-finite values")
+    m_new, se_new = _window_stats(Q[:, W:])
+    m_old, se_old = _window_stats(Q[:, :W])
+    rate, se_rate = _window_stats(np.diff(Q, axis=1))
+    d = np.stack([m_new - m_old, rate * W], axis=1)
+    tol = np.stack([np.maximum.reduce([np.full(len(names), atol), rtol * np.maximum(np.abs(m_new), np.abs(m_old)),
+                                       3 * np.hypot(se_new, se_old)]),
+                    np.maximum(atol, 3 * se_rate * W)], axis=1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = np.where(tol > 0, np.abs(d) / tol, np.where(d == 0, 0.0, np.inf))
+    k, kind = divmod(int(np.argmax(ratio)), 2)
+    return dict(name=names[k], kind=("mean", "drift")[kind], d=float(d[k, kind]), tol=float(tol[k, kind]),
+                ratio=float(ratio[k, kind]), rate=float(rate[k] / dt), unit="C/m",
+                ok=bool(np.all(np.abs(d) <= tol)))
 
 
 def history_start(hist, probes, charge_hist):
-    """First batch after which every probe and monitor history is finite (a resumed
-    run whose saved results lack some of them carries NaN there)."""
-    first = 0
-    for values in [*(hist[k] for k in probes), *charge_hist.values()]:
-        missing = np.flatnonzero(~np.isfinite(values))
-        if missing.size:
-            first = max(first, int(missing[-1]) + 1)
-    return first
+    """First batch from which every probe and monitor history is finite (a resumed run
+    whose saved results lack some of them carries NaN there)."""
+    series = [np.asarray(hist[k], dtype=float) for k in probes] + \
+             [np.asarray(v, dtype=float) for v in charge_hist.values()]
+    last_bad = [np.flatnonzero(~np.isfinite(s))[-1] + 1 for s in series if not np.isfinite(s).all()]
+    return int(max(last_bad, default=0))
