@@ -99,6 +99,10 @@ class B200Tracer:
         self._last_dev = None     # device outputs of the last call, read back on first use of .last
         self._last_host = {}
         self._ctx_dx = None
+        self._bufs = {}           # device buffers kept between calls (particles, fields, outputs)
+        self._field_host = None   # host copies of the last call's fields: unchanged fields are not re-sent
+        self._field_dev = None
+        self._packed = None       # vscale the context's FP32 field was last packed with
 
     @property
     def last(self):
@@ -118,12 +122,49 @@ class B200Tracer:
             return a.to(device=self.tdev, dtype=dtype).contiguous()
         return torch.from_numpy(np.ascontiguousarray(a, dtype=_np_dtype(dtype))).to(self.tdev, non_blocking=False)
 
+    def _buf(self, name, dtype, n):
+        """The n-element view of the tracer's own device buffer `name`, grown to at
+        least n elements when needed and kept between calls."""
+        buf = self._bufs.get(name)
+        if buf is None or buf.numel() < n:
+            buf = torch.empty(max(n, 1), dtype=dtype, device=self.tdev)
+            self._bufs[name] = buf
+        return buf[:n]
+
+    def _stage(self, name, src, dtype, n):
+        """Copies `src` (host array or tensor, any memory order) into device buffer
+        `name` (see _buf) and returns the view.  No allocation once the buffer is large
+        enough."""
+        view = self._buf(name, dtype, n)
+        if isinstance(src, torch.Tensor):
+            view.copy_(src.reshape(-1))
+        else:
+            view.copy_(torch.from_numpy(np.ascontiguousarray(src, dtype=_np_dtype(dtype)).reshape(-1)))
+        return view
+
+    def _fields(self, Ex, Ey, barrier):
+        """Device copies of the fields (and wall potential), uploaded only when they
+        differ from the previous call's; returns (EX, EY, PHI, WF, changed)."""
+        host = (Ex, Ey) + (tuple(barrier) if barrier is not None else ())
+        host = tuple(a.cpu().numpy() if isinstance(a, torch.Tensor) else np.asarray(a, dtype=np.float64)
+                     for a in host)
+        last = self._field_host
+        if last is not None and len(last) == len(host) and all(np.array_equal(a, b) for a, b in zip(host, last)):
+            return (*self._field_dev, False)
+        names = ("ex", "ey", "phi", "wface")
+        dev = [self._stage(k, a, torch.float64, a.size) for k, a in zip(names, host)]
+        dev += [None] * (4 - len(dev))
+        self._field_host = tuple(a.copy() for a in host)
+        self._field_dev = tuple(dev)
+        return (*self._field_dev, True)
+
     def _context_for(self, dx):
         # The context stores dx; a tracer serves one geometry, dx comes from p.
         if self._ctx_dx != dx:
             self.ctx.close()
             self.ctx = Context(self.vac, self.device, dx)
             self._ctx_dx = dx
+            self._packed = None
         return self.ctx
 
     # -- the reference call ------------------------------------------------------
@@ -140,7 +181,8 @@ class B200Tracer:
         if any(np.shape(v) != (nx, ny) for v in (Ex, Ey)):
             raise ValueError("field shape does not match the grid")
         spc_h = spc.cpu().numpy() if isinstance(spc, torch.Tensor) else np.asarray(spc)
-        if np.any((spc_h != 0) & (spc_h != 1)):
+        if n and (spc_h.min() < 0 or spc_h.max() > 1 if spc_h.dtype.kind in "iub"
+                  else np.any((spc_h != 0) & (spc_h != 1))):
             raise ValueError("species must be 0 (ion) or 1 (electron)")
         if barrier is not None and any(np.shape(v) != (nx, ny) for v in barrier):
             raise ValueError("wall potential shape does not match the grid")
@@ -161,20 +203,22 @@ class B200Tracer:
         stream = torch.cuda.current_stream(dev)
         sp = ctypes.c_void_p(stream.cuda_stream)
 
-        # the tracer writes particle state back (record, step budget): a caller's tensor is copied
-        X = [self._dev(v, f64) for v in (x, y, vx, vy)]
-        X = [t.clone() if isinstance(v, torch.Tensor) else t for t, v in zip(X, (x, y, vx, vy))]
-        QM = self._dev(qm, f64)
-        SPC = torch.from_numpy(np.ascontiguousarray(spc_h, dtype=np.int8)).to(dev)
-        EX, EY = self._dev(Ex, f64), self._dev(Ey, f64)
-        PHI = WF = None
-        if barrier is not None:
-            PHI, WF = self._dev(barrier[0], f64), self._dev(barrier[1], f64)
-        counts = torch.zeros((2, nx, ny), dtype=torch.int32, device=dev)
-        totals = torch.zeros(8, dtype=torch.int64, device=dev)
-        status = torch.full((n,), 3, dtype=torch.int8, device=dev)
-        hit = torch.full((n,), -1, dtype=torch.int32, device=dev)
-        steps = torch.zeros(n, dtype=torch.int32, device=dev)
+        # particles go into the tracer's own buffers (the tracer writes particle state back
+        # for record and at the step cap, so a caller's arrays are never traced in place)
+        X = [self._stage(k, v, f64, n) for k, v in zip(("x", "y", "vx", "vy"), (x, y, vx, vy))]
+        QM = self._stage("qm", qm, f64, n)
+        SPC = self._stage("spc", spc_h, torch.int8, n)
+        EX, EY, PHI, WF, fields_changed = self._fields(Ex, Ey, barrier)
+        counts = self._bufs.get("counts")
+        if counts is None:
+            counts = self._bufs["counts"] = torch.empty((2, nx, ny), dtype=torch.int32, device=dev)
+            self._bufs["totals"] = torch.empty(8, dtype=torch.int64, device=dev)
+        totals = self._bufs["totals"]
+        counts.zero_()
+        totals.zero_()
+        status = self._buf("status", torch.int8, n).fill_(3)
+        hit = self._buf("hit", torch.int32, n).fill_(-1)
+        steps = self._buf("steps", torch.int32, n).zero_()
 
         a = _capi.TraceArgs()
         a.n = n
@@ -223,8 +267,9 @@ class B200Tracer:
             keep += [SLOTS, ENDP, PATHS, PLEN]
 
         if precision == "f32" and n:
-            self.ctx.check(L.tb_set_fields(ctx.handle, _ptr(EX), _ptr(EY), _ptr(PHI), _ptr(WF),
-                                           self.vscale, sp))
+            if fields_changed or self._packed != self.vscale:
+                ctx.check(L.tb_set_fields(ctx.handle, _ptr(EX), _ptr(EY), _ptr(PHI), _ptr(WF), self.vscale, sp))
+                self._packed = self.vscale
             if rf is not None:
                 ctx.check(L.tb_set_rf_fields(ctx.handle, _ptr(RFX), _ptr(RFY), _ptr(RFP), _ptr(WF), _ptr(WAVE),
                                              len(rf["wave"]), sp))
@@ -244,10 +289,12 @@ class B200Tracer:
                 ctx.check(L.tb_trace(ctx.handle, ctypes.byref(a), _capi.PRECISION[precision], sp))
         ctx.check(L.tb_check(ctx.handle, sp))
 
-        cnt = counts.to(torch.int64).cpu().numpy()
+        cnt = counts.cpu().numpy().astype(np.int64)
         tot = totals.cpu().numpy()
         escaped = np.array([tot[0], tot[1]], dtype=np.int64)
-        lost = int((status == 3).sum().item())
+        # one launch over the whole step budget tallies the particles left live at the step
+        # cap (totals[2]); chunked launches (a stop request) count the live status instead
+        lost = int(tot[2]) if stop is None else int((status == 3).sum().item())
         self._last_dev = dict(particle_steps=int(tot[3]), status=status, hit=hit, steps=steps, precision=precision)
         if record is not None:
             host_status = self.last["status"]
