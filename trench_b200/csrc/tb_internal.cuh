@@ -30,30 +30,35 @@ __host__ __device__ __forceinline__ int tb_halo_count(int nx, int ny) {
     return (n + 1) & ~1;  // even count: whole 16-byte units for the bulk copy
 }
 
-// True if cell (ix, iy) and its 8 neighbours (x periodic, rows clipped to the grid
-// like the reference's cell lookups) are all vacuum: a move of less than one cell
-// from such a cell cannot reach a solid cell.
-__device__ __forceinline__ bool tb_interior(const uint8_t *vac, int nx, int ny, int ix, int iy) {
-    for (int a = -1; a <= 1; ++a) {
-        const int i = ix + a < 0 ? nx - 1 : (ix + a >= nx ? 0 : ix + a);
-        for (int b = -1; b <= 1; ++b) {
-            const int j = iy + b < 0 ? 0 : (iy + b > ny - 1 ? ny - 1 : iy + b);
-            if (!vac[i * ny + j]) return false;
-        }
-    }
-    return true;
+// Physical column / row of padded column pi / row pj (x periodic, rows clipped).
+__host__ __device__ __forceinline__ int tb_pad_col(int pi, int nx) {
+    return pi == 0 ? nx - 1 : (pi == nx + 1 ? 0 : pi - 1);
+}
+__host__ __device__ __forceinline__ int tb_pad_row(int pj, int ny) {
+    return pj == 0 ? 0 : (pj == ny + 1 ? ny - 1 : pj - 1);
 }
 
-// Packed tracer cell: E*vac scaled to cell units, bit 0 of ex = vacuum, bit 0 of
-// ey = interior (one-ulp perturbations of FP32 values; a flagged zero becomes the
-// smallest denormal, which flushes to zero in the tracer's arithmetic).
-__device__ __forceinline__ tb_fcell tb_pack_cell(double ex, double ey, bool vacuum, bool interior, double scale) {
+// True if the bilinear quad whose lower-left corner is padded cell (pi, pj) -- the
+// corners (pi, pj), (pi+1, pj), (pi, pj+1), (pi+1, pj+1) -- has four vacuum cells.
+// A step of less than half a cell that starts inside such a quad ends in one of its
+// corner cells, so it cannot reach a wall, and its vacuum weights sum to one.
+// Quads beyond the last corner column or row (never a particle's quad) report false.
+__device__ __forceinline__ bool tb_quad_vacuum(const uint8_t *vac, int nx, int ny, int pi, int pj) {
+    if (pi > nx || pj > ny) return false;
+    const int c0 = tb_pad_col(pi, nx) * ny, c1 = tb_pad_col(pi + 1, nx) * ny;
+    const int r0 = tb_pad_row(pj, ny), r1 = tb_pad_row(pj + 1, ny);
+    return vac[c0 + r0] && vac[c0 + r1] && vac[c1 + r0] && vac[c1 + r1];
+}
+
+// Packed tracer cell: E*vac scaled to cell units, bit 0 of ex = vacuum (one-ulp
+// perturbation of the FP32 value; a flagged zero becomes the smallest denormal, which
+// flushes to zero in the tracer's arithmetic).  Bit 0 of ey is set per padded position
+// by tb_store_packed (the quad flag).
+__device__ __forceinline__ tb_fcell tb_pack_cell(double ex, double ey, bool vacuum, double scale) {
     const double v = vacuum ? 1.0 : 0.0;
     uint32_t bx = __float_as_uint((float)(ex * v * scale));
-    uint32_t by = __float_as_uint((float)(ey * v * scale));
     bx = vacuum ? (bx | 1u) : (bx & ~1u);
-    by = interior ? (by | 1u) : (by & ~1u);
-    return tb_fcell{__uint_as_float(bx), __uint_as_float(by)};
+    return tb_fcell{__uint_as_float(bx), (float)(ey * v * scale)};
 }
 
 // Writes the packed value of cell (ix, iy) and its halo copies.
@@ -69,6 +74,26 @@ __device__ __forceinline__ void tb_store_halo(T *out, int nx, int ny, int ix, in
     if (iy == ny - 1) rs[nr++] = ny + 1;
     for (int a = 0; a < nc; ++a)
         for (int b = 0; b < nr; ++b) out[cs[a] * P + rs[b]] = v;
+}
+
+// tb_store_halo for the packed tracer field: every padded copy of cell (ix, iy) gets the
+// quad flag of its own padded position in bit 0 of ey.
+__device__ __forceinline__ void tb_store_packed(tb_fcell *out, const uint8_t *vac, int nx, int ny, int ix, int iy,
+                                                tb_fcell v) {
+    const int P = ny + 2;
+    int cs[3], rs[3], nc = 0, nr = 0;
+    cs[nc++] = ix + 1;
+    if (ix == nx - 1) cs[nc++] = 0;
+    if (ix == 0) cs[nc++] = nx + 1;
+    rs[nr++] = iy + 1;
+    if (iy == 0) rs[nr++] = 0;
+    if (iy == ny - 1) rs[nr++] = ny + 1;
+    const uint32_t by = __float_as_uint(v.ey) & ~1u;
+    for (int a = 0; a < nc; ++a)
+        for (int b = 0; b < nr; ++b) {
+            const uint32_t q = tb_quad_vacuum(vac, nx, ny, cs[a], rs[b]) ? 1u : 0u;
+            out[cs[a] * P + rs[b]] = tb_fcell{v.ex, __uint_as_float(by | q)};
+        }
 }
 
 struct tb_poisson;

@@ -329,7 +329,7 @@ __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac
     const double ex = -gx, ey = -gy;
     if (d.d_ex) { d.d_ex[c] = ex; d.d_ey[c] = ey; }
     const int v = vac[c] ? 1 : 0;
-    tb_store_halo(out, nx, ny, ix, iy, tb_pack_cell(ex, ey, v, v && tb_interior(vac, nx, ny, ix, iy), scale_e));
+    tb_store_packed(out, vac, nx, ny, ix, iy, tb_pack_cell(ex, ey, v, scale_e));
     float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!v && d.d_wface) {
         const double f = d.d_wface[c];

@@ -145,6 +145,7 @@ struct CaseView {
     int nx, ny, cells, P;
     float inv_v, cfl;
     bool barrier, tapered, first_face;
+    bool small_steps;   // cfl < 1/2: a step ends in a corner cell of its start quad
 };
 
 // One step of one particle (trench_charging_2d.py:584-650): vacuum-weighted bilinear
@@ -193,15 +194,25 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         }
         c00 = q.c00; c01 = q.c01; c10 = q.c10; c11 = q.c11;
     }
+    // A step moves at most cfl cells (|v| dt + |a| dt^2 / 2 <= cfl for the CFL dt), so with
+    // cfl below one half a step that starts inside this quad of cell centres ends in one of
+    // its four corner cells.  The quad flag (bit 0 of the lower-left corner's ey) says all
+    // four are vacuum: then the step cannot reach a wall and the vacuum weights sum to one,
+    // and both the normalisation and the end-cell checks are skipped.
+    const bool near = !(C.small_steps && (__float_as_uint(c00.ey) & 1u));
     const float ux = 1.f - tx, uy = 1.f - ty;
     const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
-    const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
     const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
     const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
+    float inv_sw = 1.f;
+    if (near) {
+        const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
+        inv_sw = __fdividef(1.f, fmaxf(sw, 1e-12f));
+    }
     float ax, ay, dt;
     const float speed = sqrtf(s.vx * s.vx + s.vy * s.vy);
     if (!RF) {
-        const float qs = __fdividef(s.qm, fmaxf(sw, 1e-12f));
+        const float qs = s.qm * inv_sw;
         ax = qs * sex;
         ay = qs * sey;
         const float acc = sqrtf(ax * ax + ay * ay);
@@ -223,7 +234,6 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         const float sys = w00 * b00.y + w10 * b10.y + w01 * b01.y + w11 * b11.y;
         const float sxm = w00 * b00.z + w10 * b10.z + w01 * b01.z + w11 * b11.z;
         const float sym = w00 * b00.w + w10 * b10.w + w01 * b01.w + w11 * b11.w;
-        const float inv_sw = __fdividef(1.f, fmaxf(sw, 1e-12f));
         const float bx = fabsf(sex) + (k.bvs * fabsf(sxs) + k.bvm * fabsf(sxm));
         const float by = fabsf(sey) + (k.bvs * fabsf(sys) + k.bvm * fabsf(sym));
         const float accel = fabsf(s.qm) * inv_sw * sqrtf(bx * bx + by * by);
@@ -240,11 +250,6 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         s.clock = c0 + (uint32_t)inc;
         s.elapsed += dt * k.t_sec;
     }
-    // the start cell is the corner on the particle's side of each centre line; its
-    // interior flag says every 8-neighbour is vacuum, so a move of < 1 cell cannot
-    // touch a wall and the end-cell and corner checks are skipped
-    const float start_ey = hx ? (hy ? c00.ey : c01.ey) : (hy ? c10.ey : c11.ey);
-    const bool near = !(__float_as_uint(start_ey) & 1u);
 
     // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
     const float vxn = s.vx + ax * dt, vyn = s.vy + ay * dt;
@@ -446,6 +451,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     C.barrier = a.d_phi != nullptr;
     C.tapered = a.tapered != 0;
     C.first_face = C.barrier || C.tapered;
+    C.small_steps = a.cfl <= 0.45;
 
     LaneState s;
     s.pid = -1;
@@ -460,9 +466,9 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     bool open = true;
 
     for (;;) {
-        // One ballot per iteration: refill empty lanes from the global queue (one
-        // atomic per warp) or leave once the queue is drained.
-        const unsigned need = __ballot_sync(FULL, s.pid < 0);
+        // Refill empty lanes from the global queue (one atomic per warp) or leave once
+        // the queue is drained.
+        unsigned need = __ballot_sync(FULL, s.pid < 0);
         if (need != 0u) {
             if (!open) {
                 if (pool != nullptr || need == FULL) break;
@@ -505,9 +511,17 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                     }
                 }
             }
+            need = __ballot_sync(FULL, s.pid < 0);
         }
-        if (s.pid < 0) continue;
-        step_particle<SMEM, RF>(k, C, s, t, q);
+        if (need == 0u) {
+            // every lane holds a particle: step them all until one of them ends, one vote
+            // per step instead of the refill bookkeeping
+            do {
+                step_particle<SMEM, RF>(k, C, s, t, q);
+            } while (__all_sync(FULL, s.pid >= 0));
+        } else if (s.pid >= 0) {
+            step_particle<SMEM, RF>(k, C, s, t, q);
+        }
     }
 
     if (pool != nullptr) {
@@ -631,7 +645,7 @@ __global__ void pack_fields_kernel(int nx, int ny, double scale_e, double scale_
     if (c >= cells) return;
     const int ix = c / ny, iy = c - ix * ny;
     const int v = vac[c] ? 1 : 0;
-    tb_store_halo(out, nx, ny, ix, iy, tb_pack_cell(ex[c], ey[c], v, v && tb_interior(vac, nx, ny, ix, iy), scale_e));
+    tb_store_packed(out, vac, nx, ny, ix, iy, tb_pack_cell(ex[c], ey[c], v, scale_e));
     float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!v && phi != nullptr) {
         const int w = (ix == 0 ? nx - 1 : ix - 1) * ny + iy;

@@ -140,39 +140,9 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
     bool open = true;
     unsigned long long my_steps = 0, my_esc_i = 0, my_esc_e = 0, my_lost = 0, my_hit_i = 0, my_hit_e = 0;
 
-    for (;;) {
-        // Refill empty lanes from the global queue (one atomic per warp).
-        const unsigned need = __ballot_sync(FULL, pid < 0);
-        if (need != 0u && open) {
-            const int leader = __ffs(need) - 1;
-            const int cnt = __popc(need);
-            unsigned long long base = 0;
-            if (lane == leader) base = atomicAdd(k.queue, (unsigned long long)cnt);
-            base = __shfl_sync(FULL, base, leader);
-            if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
-            if (pid < 0) {
-                const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
-                if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
-                    pid = (long long)idx;
-                    x = a.d_x[pid]; y = a.d_y[pid]; vx = a.d_vx[pid]; vy = a.d_vy[pid];
-                    qm = a.d_qm[pid];
-                    spc = a.d_spc[pid];
-                    steps = a.d_steps[pid];
-                    stop_at = min(a.max_steps, steps + a.step_budget);
-                    if (rf) { clock = a.d_clock[2 * pid]; elapsed = a.d_clock[2 * pid + 1]; }
-                    slot = (a.record && a.d_slots) ? a.d_slots[pid] : -1;
-                    plen = slot >= 0 ? a.d_path_len[slot] : 0;
-                    if (a.record) { xp = a.d_endpoints[2 * pid]; yp = a.d_endpoints[2 * pid + 1]; }
-                }
-            }
-        }
-        if (__ballot_sync(FULL, pid >= 0) == 0u) {
-            if (!open) break;
-            continue;
-        }
-        if (pid < 0) continue;
-
-        // ---- one step (trench_charging_2d.py:584-650) ----
+    // One step of this lane's particle (trench_charging_2d.py:584-650); on absorption,
+    // escape or the step budget the outputs are written and pid becomes -1.
+    auto step = [&]() {
         double ex, ey;
         interp(k, a.d_ex, a.d_ey, x, y, ex, ey);
         double ax = qm * ex, ay = qm * ey;
@@ -314,7 +284,48 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
             }
             pid = -1;
         }
+    };
+
+    for (;;) {
+        // Refill empty lanes from the global queue (one atomic per warp).
+        const unsigned need = __ballot_sync(FULL, pid < 0);
+        if (need != 0u && !open) break;  // queue drained: the lanes finish their particles below
+        if (need != 0u) {
+            const int leader = __ffs(need) - 1;
+            const int cnt = __popc(need);
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(k.queue, (unsigned long long)cnt);
+            base = __shfl_sync(FULL, base, leader);
+            if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
+            if (pid < 0) {
+                const unsigned long long idx = base + __popc(need & ((1u << lane) - 1u));
+                if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
+                    pid = (long long)idx;
+                    x = a.d_x[pid]; y = a.d_y[pid]; vx = a.d_vx[pid]; vy = a.d_vy[pid];
+                    qm = a.d_qm[pid];
+                    spc = a.d_spc[pid];
+                    steps = a.d_steps[pid];
+                    stop_at = min(a.max_steps, steps + a.step_budget);
+                    if (rf) { clock = a.d_clock[2 * pid]; elapsed = a.d_clock[2 * pid + 1]; }
+                    slot = (a.record && a.d_slots) ? a.d_slots[pid] : -1;
+                    plen = slot >= 0 ? a.d_path_len[slot] : 0;
+                    if (a.record) { xp = a.d_endpoints[2 * pid]; yp = a.d_endpoints[2 * pid + 1]; }
+                }
+            }
+        }
+        if (__all_sync(FULL, pid >= 0)) {
+            // every lane holds a particle: step them all until one of them ends
+            do {
+                step();
+            } while (__all_sync(FULL, pid >= 0));
+        } else if (pid >= 0) {
+            step();
+        }
     }
+    // The queue is drained: each lane runs its particle to the end with no warp-level
+    // bookkeeping, so the last, longest trajectories step at the latency of the step
+    // itself (a small batch of long trajectories is bound by exactly that).
+    while (pid >= 0) step();
 
     // Warp-reduce the per-lane tallies, one atomic per warp and counter.
 #pragma unroll
