@@ -268,6 +268,15 @@ int tb_pack_destroy(tb_pack *pack);
 const char *tb_pack_last_error(const tb_pack *pack);
 int tb_pack_set_args(tb_pack *pack, const tb_trace_args *args);
 int tb_pack_trace(tb_pack *pack, int reset, void *stream);
+/* The per-batch update (tb_step_charge then tb_step_potential) of every case of the
+ * pack in one launch per stage -- the charge update of all cases (one 8-CTA cluster
+ * per case; a case with more than 1024 surface slots runs its own), then the Green's
+ * product of all cases, then their fields -- instead of 3 launches per case.
+ * tb_pack_set_steps takes one step descriptor per case, in the pack's case order, and
+ * is synchronous; the results equal tb_step_charge + tb_step_potential per case.  No
+ * counterpart in the reference. */
+int tb_pack_set_steps(tb_pack *pack, const tb_step_desc *descs);
+int tb_pack_step(tb_pack *pack, void *stream);
 /* Synchronise `stream`, then read and clear the pack's device check flag; after
  * TB_ERR_KERNEL the batch's results are partial, as for tb_check. */
 int tb_pack_check(tb_pack *pack, void *stream);
@@ -361,6 +370,11 @@ int tb_adjoint_reverse(tb_ctx *ctx, const tb_step_desc *step, const tb_adjoint_a
 /* Measured shared-memory load bandwidth of the context's GPU (GB/s, all SMs, 8-byte
  * loads like the FP32 tracer's gathers).  A benchmark helper; synchronises the device. */
 int tb_bench_smem(tb_ctx *ctx, double *gbs);
+/* Measured random 8-byte gather bandwidth (GB/s, all SMs, read-only path) from a buffer
+ * of `bytes` (4 KiB .. 1 GiB, rounded down to a power of two) that stays in L2, like
+ * the FP32 tracer's field on grids too large for shared memory.  Allocates and frees
+ * its buffer; synchronises the device. */
+int tb_bench_l2_gather(tb_ctx *ctx, long long bytes, double *gbs);
 
 #ifdef __cplusplus
 }

@@ -264,26 +264,38 @@ def test_reverse_sweep_with_feedback_matches_the_fp64_torch_gradient(mods, recor
 def test_gradient_tracks_the_full_charging_chain(mods):
     """AR-5 workload at full size (2^20 ions + 2^20 electrons per batch, 50 batches):
     directional derivatives of the adjoint (32 feedback modes every 5 batches)
-    against central differences of the full charging chain, each run re-traced with
-    the perturbed histograms on the same Philox draws (common random numbers), steps
-    of +-10% on the 140 eV peak's bins and on the angle bins above 3 deg, the chain
-    averaged over two seeds.  Bottom-centre potential within 2%, bottom flux within
-    20% (the chain differences' own seed-to-seed spread is about 6% there); without
-    the feedback the potential's error is larger."""
+    against central differences of the full charging chain, each chain re-traced
+    with the perturbed histograms on the same Philox draws (common random numbers),
+    steps of +-10% on the 140 eV peak's bins and on the angle bins above 3 deg.
+
+    Both are Monte Carlo estimates: the chain differences over 6 seeds and the
+    adjoint over 3 recorded runs give means and standard errors, and the two means
+    must agree within 3 combined standard errors, for the bottom-centre potential
+    and the bottom ion flux.  The chain differences' own relative standard error (the
+    floor under any comparison at this sample size) is printed; without the feedback
+    term the potential's error is larger than with it."""
     torch, adjoint, inject, ChargingCase = mods
     p, eE, wE, eA, wA = adjoint.adjoint_workload()
     B = p.n_batches
-    case = ChargingCase(p, precision="f32", max_batches=B)
-    hist = adjoint.AdjointRecorder(case, eE, wE, eA, wA, seed=21).run(B)
     f64 = torch.float64
-    grads = {}
-    for fb in (True, False):
-        for name in ("phi", "flux"):
-            gE = torch.tensor(wE, dtype=f64, device=case.dev, requires_grad=True)
-            gA = torch.tensor(wA, dtype=f64, device=case.dev, requires_grad=True)
-            out = adjoint.objectives(hist, gE, gA, feedback=fb)
-            (out["phi_bottom"] if name == "phi" else out["ratio_i_bottom"][-1]).backward()
-            grads[fb, name] = (gE.grad.cpu().numpy(), gA.grad.cpu().numpy())
+    cE = 0.5 * (eE[1:] + eE[:-1])
+    cA = np.degrees(0.5 * (eA[1:] + eA[:-1]))
+    directions = ((np.where(np.abs(cE - 140) < 15, 1.0, 0.0), np.zeros_like(wA)),
+                  (np.zeros_like(wE), np.where(cA > 3, 1.0, 0.0)))
+
+    def adjoint_derivatives(seed):
+        case = ChargingCase(p, precision="f32", max_batches=B)
+        hist = adjoint.AdjointRecorder(case, eE, wE, eA, wA, seed=seed).run(B)
+        out = {}
+        for fb in (True, False):
+            for name in ("phi", "flux"):
+                gE = torch.tensor(wE, dtype=f64, device=case.dev, requires_grad=True)
+                gA = torch.tensor(wA, dtype=f64, device=case.dev, requires_grad=True)
+                o = adjoint.objectives(hist, gE, gA, feedback=fb)
+                (o["phi_bottom"] if name == "phi" else o["ratio_i_bottom"][-1]).backward()
+                g = (gE.grad.cpu().numpy(), gA.grad.cpu().numpy())
+                out[fb, name] = [float(np.dot(g[0], wE * vE) + np.dot(g[1], wA * vA)) for vE, vA in directions]
+        return out
 
     def chain(wE_, wA_, seed):
         c = ChargingCase(p, precision="f32", max_batches=B)
@@ -295,14 +307,17 @@ def test_gradient_tracks_the_full_charging_chain(mods):
         h = c.history()
         return np.array([h["bottom center"][-1], h["ratio_i_bottom"][-1]])
 
-    cE = 0.5 * (eE[1:] + eE[:-1])
-    cA = np.degrees(0.5 * (eA[1:] + eA[:-1]))
+    adj = [adjoint_derivatives(s) for s in (21, 31, 41)]
     h = 0.1
-    for vE, vA in ((np.where(np.abs(cE - 140) < 15, 1.0, 0.0), np.zeros_like(wA)),
-                   (np.zeros_like(wE), np.where(cA > 3, 1.0, 0.0))):
-        fd = np.mean([(chain(wE * (1 + h * vE), wA * (1 + h * vA), s) - chain(wE * (1 - h * vE), wA * (1 - h * vA), s))
-                      / (2 * h) for s in (21, 22)], axis=0)
-        adj = {k: float(np.dot(g[0], wE * vE) + np.dot(g[1], wA * vA)) for k, g in grads.items()}
-        assert abs(adj[True, "phi"] - fd[0]) <= 0.02 * abs(fd[0]), (adj, fd)
-        assert abs(adj[True, "flux"] - fd[1]) <= 0.20 * abs(fd[1]), (adj, fd)
-        assert abs(adj[False, "phi"] - fd[0]) > abs(adj[True, "phi"] - fd[0]), (adj, fd)
+    for d, (vE, vA) in enumerate(directions):
+        fd = np.array([(chain(wE * (1 + h * vE), wA * (1 + h * vA), s) - chain(wE * (1 - h * vE), wA * (1 - h * vA), s))
+                       / (2 * h) for s in range(21, 27)])
+        fd_mean, fd_se = fd.mean(axis=0), fd.std(axis=0, ddof=1) / np.sqrt(len(fd))
+        for j, name in enumerate(("phi", "flux")):
+            a = np.array([r[True, name][d] for r in adj])
+            a_mean, a_se = a.mean(), a.std(ddof=1) / np.sqrt(len(a))
+            print(f"direction {d} {name}: adjoint {a_mean:.6g} +- {a_se:.2g}, chain {fd_mean[j]:.6g} +- {fd_se[j]:.2g} "
+                  f"(chain relative standard error {fd_se[j] / abs(fd_mean[j]):.2%})")
+            assert abs(a_mean - fd_mean[j]) <= 3 * np.hypot(a_se, fd_se[j]), (name, d, a, fd[:, j])
+        frozen = np.mean([r[False, "phi"][d] for r in adj])
+        assert abs(frozen - fd_mean[0]) > abs(np.mean([r[True, "phi"][d] for r in adj]) - fd_mean[0])

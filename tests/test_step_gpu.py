@@ -189,9 +189,11 @@ def test_fp64_batch_loop_matches_reference_cfg1_full_run(case_cls):
 def test_fp32_batch_loop_tracks_reference_cfg1_full_run(case_cls):
     """Same 30-batch run with the FP32 tracer: per-batch bottom ion flux within
     3 sigma of the reference (counting noise of the batch), the final surface
-    charge's total within 1%, and the potential within 1e-3 V of the reference
-    wherever the two runs deposited the same charge history up to noise (max error
-    over the grid within 2% of the potential swing)."""
+    charge's total within 1%, and the final potential within 2% of its swing on
+    every cell.  After the first hit that differs from the FP64 run the two runs
+    are different Monte Carlo samples of the same charging, so their potentials
+    differ by the charging noise; the 1e-3 V bar holds for one batch from a common
+    charge (test_accuracy_gpu.py)."""
     g = load_golden("run_cfg1_30.npz")
     p = g["p"]
     case = case_cls(p, precision="f32", green="f64")

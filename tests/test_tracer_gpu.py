@@ -100,13 +100,23 @@ def test_f32_hits_agree_with_fp64_oracle(tracers, name):
     want = OT.trace_detail(*parts(g)[:5], g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g))
     same = (t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])
     n = len(same)
-    assert same.mean() >= 0.99, f"agreement {same.mean():.5f}"
     # counts restricted to agreeing particles are identical by construction; the
     # totals differ by at most the disagreeing particles
     total = got[0].sum() + got[1].sum() + got[2].sum() + got[3]
     assert total == n
     diff = np.abs(got[0] - OT.counts_from_detail(want, g["spc"], g["solid"].shape)[0]).sum()
     assert diff <= 2 * (~same).sum()
+    # the 99.9 % bar: on the fixture when it holds 2^16 particles or more, else on a seeded
+    # sample of 2^15 per species through the fixture's geometry and fields
+    if n >= 1 << 16:
+        agree = same.mean()
+    else:
+        p = g["p"]
+        x, y, vx, vy, qm, spc = inject.inject(p, 1 << 15, g["solid"].shape[1], np.random.default_rng(321))
+        t(x, y, vx, vy, qm, spc, g["Ex"], g["Ey"], ~g["solid"], p, barrier(g))
+        want = OT.trace_detail(x, y, vx, vy, qm, g["Ex"], g["Ey"], ~g["solid"], p, barrier(g))
+        agree = ((t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])).mean()
+    assert agree >= 0.999, f"agreement {agree:.5f}"
 
 
 def test_f32_large_sample_agreement_and_bottom_flux(tracers):
@@ -143,7 +153,7 @@ def test_f32_rf_hits_agree_with_fp64_oracle(tracers):
     want = OT.trace_detail(*parts(g)[:5], g["Ex"], g["Ey"], ~g["solid"], g["p"], barrier(g), rf=rf_of(g))
     same = (t.last["status"] == want["status"]) & (t.last["hit"] == want["hit"])
     print(f"FP32 RF vs FP64 oracle: {same.mean():.5f} of {len(same)}")
-    assert same.mean() >= 0.99, f"agreement {same.mean():.5f}"
+    assert same.mean() >= 0.999, f"agreement {same.mean():.5f}"
     assert got[0].sum() + got[1].sum() + got[2].sum() + got[3] == len(same)
 
 

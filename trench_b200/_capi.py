@@ -142,6 +142,7 @@ SIGNATURES = {
     "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_monitors": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp, _vp, ctypes.c_int, _vp, _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
+    "tb_bench_l2_gather": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.POINTER(_dbl)]),
     "tb_inject": (ctypes.c_int, [_vp, ctypes.POINTER(InjectArgs), _vp]),
     "tb_philox_fill": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int, _vp, _vp]),
     "tb_pack_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),
@@ -150,6 +151,8 @@ SIGNATURES = {
     "tb_pack_set_args": (ctypes.c_int, [_vp, ctypes.POINTER(TraceArgs)]),
     "tb_pack_trace": (ctypes.c_int, [_vp, ctypes.c_int, _vp]),
     "tb_pack_check": (ctypes.c_int, [_vp, _vp]),
+    "tb_pack_set_steps": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc)]),
+    "tb_pack_step": (ctypes.c_int, [_vp, _vp]),
     "tb_tally": (ctypes.c_int, [_vp, ctypes.POINTER(TallyArgs), _vp]),
     "tb_adjoint_forward": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), ctypes.POINTER(AdjointArgs), _vp]),
     "tb_adjoint_reverse": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), ctypes.POINTER(AdjointArgs), _vp, _vp,

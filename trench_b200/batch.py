@@ -2,8 +2,9 @@
 
 All cases' particles are traced by one persistent launch (``tb_pack_trace``: CTAs
 move between cases by remaining work, so uneven cases share every SM); the
-per-case charge, leakage, conductor, potential and field updates follow, and a
-whole batch of all cases can be captured as one CUDA graph.  The reference runs
+charge, leakage, conductor, potential and field updates of all cases follow as one
+launch per stage (``tb_pack_step``), and a whole batch of all cases can be
+captured as one CUDA graph.  The reference runs
 such a sweep as one ``run()`` per case (trench_charging_2d.py:1045).
 
 ``sweep_params`` draws the sweep workload of uneven cases (widths, depths,
@@ -71,6 +72,10 @@ class ChargingBatch:
         self.n_loaded = [0] * len(self.cases)
         self._graph = None
         self._args_for = None
+        descs = (_capi.StepDesc * len(self.cases))(*[c._desc for c in self.cases])
+        self._check(L.tb_pack_set_steps(self.pack, descs))
+        self.per_case_update = False   # True: 3 launches per case (tb_step_charge, tb_step_potential)
+        self.trace_events = None       # optional (start, end) CUDA events around the tracer launch
 
     def _check(self, code):
         if code != _capi.TB_OK:
@@ -111,10 +116,18 @@ class ChargingBatch:
         L = _capi.lib()
         self._set_args()
         s = ctypes.c_void_p(torch.cuda.current_stream(self.dev).cuda_stream)
+        ev = self.trace_events
+        if ev is not None:
+            ev[0].record()
         self._check(L.tb_pack_trace(self.pack, 1, s))
-        for c in self.cases:
-            c.ctx.check(L.tb_step_charge(c.ctx.handle, ctypes.byref(c._desc), s))
-            c.ctx.check(L.tb_step_potential(c.ctx.handle, ctypes.byref(c._desc), s))
+        if ev is not None:
+            ev[1].record()
+        if self.per_case_update:
+            for c in self.cases:
+                c.ctx.check(L.tb_step_charge(c.ctx.handle, ctypes.byref(c._desc), s))
+                c.ctx.check(L.tb_step_potential(c.ctx.handle, ctypes.byref(c._desc), s))
+        else:
+            self._check(L.tb_pack_step(self.pack, s))
 
     def capture(self):
         self._set_args()

@@ -150,6 +150,26 @@ int tb_launch_pack_fields(tb_ctx *ctx, const double *ex, const double *ey, const
 int tb_launch_pack_rf_fields(tb_ctx *ctx, const double *rf_ex, const double *rf_ey, const double *rf_phi,
                              const double *wface, const double *wave, int n_phase, cudaStream_t s);
 
+// One case's per-batch update as the case-pack update kernels read it (device array,
+// one entry per case): its step descriptor, grid and packed tracer-field outputs.
+struct tb_pack_step_entry {
+    tb_step_desc d;
+    int nx, ny;
+    const uint8_t *vac;
+    double scale_e, scale_phi;
+    tb_fcell *field;
+    float4 *bar;
+    int *err;
+};
+
+// Per-batch update of every case of a pack (tb_step.cu): set once from one descriptor
+// per case, then run as one launch per stage.
+struct tb_pack_steps;
+int tb_pack_steps_set(tb_pack_steps **ps, int n, tb_ctx *const *ctxs, const tb_step_desc *descs, char *err,
+                      size_t errlen);
+int tb_pack_steps_run(tb_pack_steps *ps, cudaStream_t s, char *err, size_t errlen);
+void tb_pack_steps_free(tb_pack_steps *ps);
+
 // Deposits one particle into counts[key] (key = species * cells + cell).  Warp-aggregated:
 // the lanes of the warp that deposit into the same key at this point add once, with
 // the number of such lanes.  The counts are integers, so the result is exact and

@@ -20,6 +20,9 @@
 #include <cooperative_groups.h>
 #include <math.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "tb_internal.cuh"
 
 namespace cg = cooperative_groups;
@@ -97,12 +100,11 @@ __global__ void __launch_bounds__(ONE_BLOCK) k_deposit(const tb_step_desc d, int
     }
 }
 
-// y = A x with A row-major (rows, cols); one warp per row, FP64 accumulation.
+// y = A x with A row-major (rows, cols); one warp per row, FP64 accumulation.  Row
+// `warp` of the product; with `scatter`, y[scatter[warp]] = y0[scatter[warp]] + row.
 template <typename T>
-__global__ void k_gemv(int rows, int cols, const T *A, const double *x, double *y, const double *y0,
-                       const int32_t *scatter) {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= rows) return;
+__device__ __forceinline__ void gemv_row(int warp, int lane, int cols, const T *A, const double *x, double *y,
+                                         const double *y0, const int32_t *scatter) {
     const T *a = A + (size_t)warp * cols;
     double acc = 0.0;
     for (int c = lane; c < cols; c += 32) acc += (double)a[c] * x[c];
@@ -115,6 +117,14 @@ __global__ void k_gemv(int rows, int cols, const T *A, const double *x, double *
             y[warp] = acc;
         }
     }
+}
+
+template <typename T>
+__global__ void k_gemv(int rows, int cols, const T *A, const double *x, double *y, const double *y0,
+                       const int32_t *scatter) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= rows) return;
+    gemv_row<T>(warp, lane, cols, A, x, y, y0, scatter);
 }
 
 // K3: leakage result, conductor step, history scalars.
@@ -168,8 +178,7 @@ __global__ void __launch_bounds__(ONE_BLOCK) k_finish(const tb_step_desc d, cons
 constexpr int FUSED_CTAS = 8;
 constexpr int FUSED_MAX_M = 1024;
 
-__global__ void __cluster_dims__(FUSED_CTAS, 1, 1) __launch_bounds__(ONE_BLOCK)
-    k_charge_fused(const tb_step_desc d, int ncell, int *err) {
+__device__ __forceinline__ void charge_fused(const tb_step_desc &d, int ncell, int *err) {
     cg::cluster_group cl = cg::this_cluster();
     const int rank = (int)cl.block_rank();
     __shared__ double sh[32];
@@ -268,6 +277,11 @@ __global__ void __cluster_dims__(FUSED_CTAS, 1, 1) __launch_bounds__(ONE_BLOCK)
     cl.sync();  // block 0 has read every block's partial sums before any block exits
 }
 
+__global__ void __cluster_dims__(FUSED_CTAS, 1, 1) __launch_bounds__(ONE_BLOCK)
+    k_charge_fused(const tb_step_desc d, int ncell, int *err) {
+    charge_fused(d, ncell, err);
+}
+
 // Charge monitors of the history (trench_charging_2d.py:871-874, 1281-1285): for each
 // monitor r, dx^2 sum_s w[r][s] x (|rho_s| if absolute[r] else rho_s) into row
 // *d_batch of out.  Charge only sits on surface slots, so the monitors' cell sets are
@@ -291,9 +305,8 @@ __global__ void k_monitors(const tb_step_desc d, const double *w, const uint8_t 
 
 // K5: E = -grad phi over vacuum neighbours (trench_charging_2d.py:429-454), the
 // packed FP32 tracer field, the per-face wall barrier and the probe history.
-__global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac, double scale_e, double scale_phi,
-                        tb_fcell *out, float4 *bar) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void field_cell(const tb_step_desc &d, int c, int nx, int ny, const uint8_t *vac,
+                                           double scale_e, double scale_phi, tb_fcell *out, float4 *bar) {
     const int n = nx * ny;
     if (c == 0) {
         const int row = *d.d_batch;
@@ -339,6 +352,37 @@ __global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac
         b.w = iy < ny - 1 ? (float)(f * (pc - phi[c + 1]) * scale_phi) : 0.f;
     }
     bar[c] = b;
+}
+
+__global__ void k_field(const tb_step_desc d, int nx, int ny, const uint8_t *vac, double scale_e, double scale_phi,
+                        tb_fcell *out, float4 *bar) {
+    field_cell(d, blockIdx.x * blockDim.x + threadIdx.x, nx, ny, vac, scale_e, scale_phi, out, bar);
+}
+
+// ---- the same update for every case of a pack, one launch per stage ----------------
+// Case = blockIdx.y; each case's descriptor, grid and packed-field outputs in one entry.
+constexpr int PACK_THREADS = 256;
+
+__global__ void __cluster_dims__(FUSED_CTAS, 1, 1) __launch_bounds__(ONE_BLOCK)
+    k_pack_charge(const tb_pack_step_entry *E) {
+    const tb_pack_step_entry &e = E[blockIdx.y];
+    charge_fused(e.d, e.nx * e.ny, e.err);
+}
+
+__global__ void __launch_bounds__(PACK_THREADS) k_pack_green(const tb_pack_step_entry *E) {
+    const tb_pack_step_entry &e = E[blockIdx.y];
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= e.d.n_rows) return;
+    if (e.d.d_green)
+        gemv_row<float>(warp, lane, e.d.m, e.d.d_green, e.d.d_rho_s, e.d.d_phi, e.d.d_ext, e.d.d_rows);
+    else
+        gemv_row<double>(warp, lane, e.d.m, e.d.d_green64, e.d.d_rho_s, e.d.d_phi, e.d.d_ext, e.d.d_rows);
+}
+
+__global__ void __launch_bounds__(PACK_THREADS) k_pack_field(const tb_pack_step_entry *E) {
+    const tb_pack_step_entry &e = E[blockIdx.y];
+    field_cell(e.d, blockIdx.x * blockDim.x + threadIdx.x, e.nx, e.ny, e.vac, e.scale_e, e.scale_phi, e.field,
+               e.bar);
 }
 
 }  // namespace
@@ -411,3 +455,109 @@ extern "C" int tb_step_monitors(tb_ctx *ctx, const tb_step_desc *d, const double
     return TB_OK;
 }
 
+
+// ---- case packs: the per-batch update of every case, one launch per stage ---------------
+
+struct tb_pack_steps {
+    int n = 0;
+    std::vector<tb_ctx *> ctxs;
+    std::vector<tb_step_desc> descs;
+    std::vector<int> own_charge;     // cases whose charge update runs alone (m > FUSED_MAX_M)
+    tb_pack_step_entry *d_entries = nullptr;
+    tb_pack_step_entry *d_fused = nullptr;  // the cases of the batched charge launch
+    int n_fused = 0;
+    int green_blocks = 0, field_blocks = 0;
+};
+
+void tb_pack_steps_free(tb_pack_steps *ps) {
+    if (!ps) return;
+    cudaFree(ps->d_entries);
+    cudaFree(ps->d_fused);
+    delete ps;
+}
+
+int tb_pack_steps_set(tb_pack_steps **out, int n, tb_ctx *const *ctxs, const tb_step_desc *descs, char *err,
+                      size_t errlen) {
+    auto fail = [&](const char *msg) {
+        snprintf(err, errlen, "%s", msg);
+        return TB_ERR_ARG;
+    };
+    if (n < 1 || n > 65535 || !ctxs || !descs) return fail("tb_pack_set_steps: needs 1 to 65535 cases");
+    std::vector<tb_pack_step_entry> entries(n), fused;
+    std::vector<int> own;
+    int green_blocks = 0, field_blocks = 0;
+    const int wpb = PACK_THREADS / 32;
+    for (int i = 0; i < n; ++i) {
+        const tb_step_desc &d = descs[i];
+        const tb_ctx *c = ctxs[i];
+        if (d.m < 1 || !d.d_surf || !d.d_sflag || !d.d_rho_s || !d.d_rho_prev || !d.d_work || !d.d_counts ||
+            !d.d_totals || !d.d_batch || !d.d_hist || d.hist_cols < 6 || !(d.dx > 0) || !(d.bottom_norm > 0) ||
+            !(d.n_per_batch > 0) || d.n_rows < 1 || !d.d_rows || (!d.d_green && !d.d_green64) || !d.d_ext ||
+            !d.d_phi || !(d.vscale > 0))
+            return fail("tb_pack_set_steps: incomplete step descriptor");
+        if (d.floating && (!d.d_g_s || !(d.C_cond > 0)))
+            return fail("tb_pack_set_steps: floating conductor needs g_s and C_cond");
+        if (d.d_leak_M && !(d.dt_batch > 0 && d.leak_norm > 0))
+            return fail("tb_pack_set_steps: leakage needs dt_batch and leak_norm");
+        tb_pack_step_entry &e = entries[i];
+        e.d = d;
+        e.nx = c->nx;
+        e.ny = c->ny;
+        e.vac = c->d_vac;
+        e.scale_e = c->dx / (d.vscale * d.vscale);
+        e.scale_phi = 1.0 / (d.vscale * d.vscale);
+        e.field = c->d_field;
+        e.bar = c->d_barrier;
+        e.err = c->d_err;
+        if (d.m <= FUSED_MAX_M) fused.push_back(e);
+        else own.push_back(i);
+        green_blocks = std::max(green_blocks, (d.n_rows + wpb - 1) / wpb);
+        field_blocks = std::max(field_blocks, (c->nx * c->ny + PACK_THREADS - 1) / PACK_THREADS);
+    }
+    tb_pack_steps *ps = new tb_pack_steps();
+    cudaError_t e = cudaSetDevice(ctxs[0]->device);
+    if (e == cudaSuccess) e = cudaMalloc(&ps->d_entries, sizeof(tb_pack_step_entry) * n);
+    if (e == cudaSuccess && !fused.empty()) e = cudaMalloc(&ps->d_fused, sizeof(tb_pack_step_entry) * fused.size());
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ps->d_entries, entries.data(), sizeof(tb_pack_step_entry) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !fused.empty())
+        e = cudaMemcpy(ps->d_fused, fused.data(), sizeof(tb_pack_step_entry) * fused.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        tb_pack_steps_free(ps);
+        snprintf(err, errlen, "tb_pack_set_steps: %s", cudaGetErrorString(e));
+        return TB_ERR_CUDA;
+    }
+    ps->n = n;
+    ps->ctxs.assign(ctxs, ctxs + n);
+    ps->descs.assign(descs, descs + n);
+    ps->own_charge = own;
+    ps->n_fused = (int)fused.size();
+    ps->green_blocks = green_blocks;
+    ps->field_blocks = field_blocks;
+    tb_pack_steps_free(*out);
+    *out = ps;
+    return TB_OK;
+}
+
+int tb_pack_steps_run(tb_pack_steps *ps, cudaStream_t s, char *err, size_t errlen) {
+    if (ps->n_fused > 0) k_pack_charge<<<dim3(FUSED_CTAS, ps->n_fused), ONE_BLOCK, 0, s>>>(ps->d_fused);
+    for (int i : ps->own_charge) {
+        const int code = tb_step_charge(ps->ctxs[i], &ps->descs[i], s);
+        if (code != TB_OK) {
+            snprintf(err, errlen, "%s", ps->ctxs[i]->err);
+            return code;
+        }
+    }
+    k_pack_green<<<dim3(ps->green_blocks, ps->n), PACK_THREADS, 0, s>>>(ps->d_entries);
+    k_pack_field<<<dim3(ps->field_blocks, ps->n), PACK_THREADS, 0, s>>>(ps->d_entries);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        snprintf(err, errlen, "tb_pack_step: %s", cudaGetErrorString(e));
+        return TB_ERR_CUDA;
+    }
+    for (int i = 0; i < ps->n; ++i) {
+        ps->ctxs[i]->vscale = ps->descs[i].vscale;
+        ps->ctxs[i]->fields_ready = 1;
+    }
+    return TB_OK;
+}

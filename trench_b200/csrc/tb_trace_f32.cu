@@ -961,6 +961,7 @@ struct tb_pack {
     size_t launch_shm = 0;
     int num_sms = 0;
     int ready = 0;
+    tb_pack_steps *steps = nullptr;  // per-batch update of every case (tb_pack_set_steps)
     char err[512] = {0};
 };
 
@@ -1034,6 +1035,7 @@ extern "C" int tb_pack_destroy(tb_pack *p) {
     cudaFree(p->d_cases);
     cudaFree(p->d_queues);
     cudaFree(p->d_err);
+    tb_pack_steps_free(p->steps);
     delete p;
     return TB_OK;
 }
@@ -1105,6 +1107,23 @@ extern "C" int tb_pack_trace(tb_pack *p, int reset, void *stream) {
         trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, p->launch_shm, s>>>(p->d_cases, p->n, p->d_err);
     e = cudaGetLastError();
     if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
+    return TB_OK;
+}
+
+extern "C" int tb_pack_set_steps(tb_pack *p, const tb_step_desc *descs) {
+    if (!p || !descs) return TB_ERR_ARG;
+    const int code = tb_pack_steps_set(&p->steps, p->n, p->ctxs.data(), descs, p->err, sizeof(p->err));
+    if (code != TB_OK) return tb_fail(nullptr, code, "%s", p->err);
+    return TB_OK;
+}
+
+extern "C" int tb_pack_step(tb_pack *p, void *stream) {
+    if (!p) return TB_ERR_ARG;
+    if (!p->steps) return pack_fail(p, TB_ERR_ARG, "tb_pack_step: call tb_pack_set_steps first");
+    cudaError_t e = cudaSetDevice(p->device);
+    if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
+    const int code = tb_pack_steps_run(p->steps, (cudaStream_t)stream, p->err, sizeof(p->err));
+    if (code != TB_OK) return tb_fail(nullptr, code, "%s", p->err);
     return TB_OK;
 }
 

@@ -610,6 +610,43 @@ class ChargingCase:
         r[self.S] = self.rho_s.cpu().numpy()
         return r.reshape(self.nx, self.ny)
 
+    def compare_precisions(self, batch):
+        """The FP32 tracer against the FP64 one on one batch from the case's current state:
+        the same particles (host arrays x, y, vx, vy, qm, spc) traced by both kernels from
+        the same charge, each followed by the same charge update; the case is left as it
+        was.  Returns the per-particle agreement of status and absorbing cell, the bottom
+        ion-flux ratio of the batch under each (difference in % and in units of its
+        counting noise) and the largest potential difference after the update over every
+        cell (V)."""
+        ck = self.checkpoint()
+        n = len(batch[0])
+        saved_hit, saved_precision = self.hit, self.precision
+        self.hit = torch.full((self.capacity,), -1, dtype=torch.int32, device=self.dev)
+        out = {}
+        try:
+            for prec in ("f32", "f64"):
+                self.restore(ck)
+                self.precision = prec
+                self.hit.fill_(-1)
+                self.load(*batch)
+                self.step(n)
+                torch.cuda.synchronize(self.dev)
+                out[prec] = dict(status=self.status[:n].cpu().numpy(), hit=self.hit[:n].cpu().numpy(),
+                                 ratio=float(self.history()["ratio_i_bottom"][-1]), phi=self.full_potential())
+        finally:
+            self.precision = saved_precision
+            self.hit = saved_hit
+            self.restore(ck)
+        a, b = out["f32"], out["f64"]
+        same = (a["status"] == b["status"]) & (a["hit"] == b["hit"])
+        norm = self.p.n_per_batch * (self.b1 - self.b0) / self.nx
+        sigma = np.sqrt(max(b["ratio"] * norm, 1.0)) / norm
+        return {"particles": n, "hit_agreement": float(same.mean()), "differing": int((~same).sum()),
+                "ratio_i_bottom": {"f32": a["ratio"], "f64": b["ratio"],
+                                   "error_pct": 100.0 * abs(a["ratio"] - b["ratio"]) / max(abs(b["ratio"]), 1e-300),
+                                   "error_sigma": abs(a["ratio"] - b["ratio"]) / sigma},
+                "potential_max_abs_diff_V": float(np.abs(a["phi"] - b["phi"]).max())}
+
     def full_potential(self):
         """phi on every cell: solve(-rho/eps0) + external (trench_charging_2d.py:1268)."""
         rho = self.rho()
