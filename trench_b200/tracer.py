@@ -190,10 +190,13 @@ class B200Tracer:
             raise ValueError("probe_trajectories must be at least 1")
         if rf is not None:
             _validate_rf(rf, n, self.vac.shape)
-        with torch.cuda.device(self.device):
-            return self._trace(x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf)
+        return self._trace(x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf)
 
     def _trace(self, x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf):
+        with torch.cuda.device(self.device):
+            return self._trace_on_device(x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf)
+
+    def _trace_on_device(self, x, y, vx, vy, qm, spc_h, Ex, Ey, p, barrier, record, stop, rf):
         L = _capi.lib()
         ctx = self._context_for(float(p.dx))
         n = len(x)
