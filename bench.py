@@ -344,6 +344,7 @@ def run_b200(args, p):
     value = particles / (total_ms / 1000.0)
     peaks = measured_peaks()
     hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_source = "of measured (MEASURED_PEAKS.json)" if "hbm_gbs" in peaks else "of fallback (6.65 TB/s)"
     # Tracer roofline: algorithmic bytes = 36 B per particle-step (4 bilinear corners of
     # Ex, Ey, vacuum in FP32) + 28 B per particle (SoA load + status/hit store).
     alg_bytes = [36.0 * s + 28.0 * n for s in steps_per_batch]
@@ -356,6 +357,7 @@ def run_b200(args, p):
             "peak_source": "measured shared-memory load bandwidth (bench microkernel)",
             "traffic": (traffic[0] * n + traffic[1] * mean_steps) if traffic else None,
             "hbm_peak_gbs": hbm, "hbm_frac_of_measured": (achieved / hbm) if hbm else None,
+            "hbm_peak_source": hbm_source,
             "kernel": "trace_f32_kernel", "trace_ms_per_launch": float(np.mean(trace_ms)),
             "particle_steps_per_launch": mean_steps,
             "particle_steps_per_s": float(np.mean([s / (t / 1000.0) for s, t in zip(steps_per_batch, trace_ms)]))}
