@@ -659,11 +659,11 @@ def large_measure(steps, warmup, n_per_species=1 << 23, tracer_shape="auto", cpu
            "roofline": {"bound": "l2", "kernel": "trace_f32_kernel (global-memory field)", "achieved": achieved,
                         "peak": l2.value if l2_ok else None, "unit": "GB/s",
                         "frac": achieved / l2.value if l2_ok and l2.value > 0 else None,
-                        "peak_source": f"measured random 8-byte gather bandwidth from an L2-resident "
+                        "peak_source": f"measured random 32-byte sector gathers from an L2-resident "
                                        f"{field_bytes / 2**20:.1f} MiB buffer (bench microkernel)",
                         "note": "36 B per particle-step + 28 B per particle over the tracer launch; a lane reuses "
-                                "its four corners while it stays in one cell quad, so fewer bytes are loaded "
-                                "than counted"},
+                                "its four corners while it stays in one cell quad, and two of them share a "
+                                "sector, so fewer sectors are fetched than the bytes counted"},
            "l2": "flushed between timed steps (256 MiB write)", "clocks": clk,
            # per step: injection, tracer, deposit, leakage GEMV, finish (m > 1024: unfused charge
            # update), Green's GEMV, field, monitors

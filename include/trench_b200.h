@@ -370,9 +370,9 @@ int tb_adjoint_reverse(tb_ctx *ctx, const tb_step_desc *step, const tb_adjoint_a
 /* Measured shared-memory load bandwidth of the context's GPU (GB/s, all SMs, 8-byte
  * loads like the FP32 tracer's gathers).  A benchmark helper; synchronises the device. */
 int tb_bench_smem(tb_ctx *ctx, double *gbs);
-/* Measured random 8-byte gather bandwidth (GB/s, all SMs, read-only path) from a buffer
- * of `bytes` (4 KiB .. 1 GiB, rounded down to a power of two) that stays in L2, like
- * the FP32 tracer's field on grids too large for shared memory.  Allocates and frees
+/* Measured random gather bandwidth of whole 32-byte sectors (GB/s, all SMs, read-only
+ * path) from a buffer of `bytes` (4 KiB .. 1 GiB, rounded down to a power of two) that
+ * stays in L2, like the FP32 tracer's field on grids too large for shared memory.  Allocates and frees
  * its buffer; synchronises the device. */
 int tb_bench_l2_gather(tb_ctx *ctx, long long bytes, double *gbs);
 

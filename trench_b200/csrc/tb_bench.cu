@@ -1,7 +1,7 @@
 // Bandwidth microbenchmarks for the FP32 tracer's roofline denominators: shared-memory
-// loads (its bilinear gathers are 8-byte shared-memory loads) and random 8-byte
-// gathers from an L2-resident global buffer (the path of grids too large for shared
-// memory).
+// loads (its bilinear gathers are 8-byte shared-memory loads) and random 32-byte
+// sector gathers from an L2-resident global buffer (the path of grids too large for
+// shared memory).
 #include "tb_internal.cuh"
 
 namespace {
@@ -26,18 +26,20 @@ __global__ void __launch_bounds__(1024, 1) k_smem_read(int words, int iters, flo
     if (acc.x == -1.f) sink[blockIdx.x] = acc.y;  // keeps the loads live
 }
 
-// Random 8-byte gathers from a global buffer small enough to stay in L2 (read-only
-// path, as the FP32 tracer's global-memory field): four independent chains per thread.
-__global__ void __launch_bounds__(1024, 1) k_l2_gather(const float2 *__restrict__ buf, unsigned mask, int iters,
+// Random gathers of whole 32-byte sectors (two 16-byte loads each, the unit in which L2
+// serves a request) from a global buffer small enough to stay in L2, read-only path as
+// the FP32 tracer's global-memory field; four independent chains per thread.
+__global__ void __launch_bounds__(1024, 1) k_l2_gather(const float4 *__restrict__ buf, unsigned mask, int iters,
                                                        float *sink) {
     unsigned i0 = (blockIdx.x * blockDim.x + threadIdx.x) * 2654435761u, i1 = i0 ^ 0x9e3779b9u,
              i2 = i0 ^ 0x7f4a7c15u, i3 = i0 ^ 0x94d049bbu;
     float acc = 0.f;
-#pragma unroll 4
+#pragma unroll 2
     for (int it = 0; it < iters; ++it) {
-        const float2 a = __ldg(buf + (i0 & mask)), b = __ldg(buf + (i1 & mask));
-        const float2 c = __ldg(buf + (i2 & mask)), d = __ldg(buf + (i3 & mask));
-        acc += (a.x + b.x) + (c.y + d.y);
+        const unsigned s0 = 2u * (i0 & mask), s1 = 2u * (i1 & mask), s2 = 2u * (i2 & mask), s3 = 2u * (i3 & mask);
+        const float4 a0 = __ldg(buf + s0), a1 = __ldg(buf + s0 + 1), b0 = __ldg(buf + s1), b1 = __ldg(buf + s1 + 1);
+        const float4 c0 = __ldg(buf + s2), c1 = __ldg(buf + s2 + 1), d0 = __ldg(buf + s3), d1 = __ldg(buf + s3 + 1);
+        acc += ((a0.x + a1.w) + (b0.y + b1.z)) + ((c0.z + c1.y) + (d0.w + d1.x));
         i0 = i0 * 1664525u + 1013904223u;
         i1 = i1 * 1664525u + 1013904223u;
         i2 = i2 * 1664525u + 1013904223u;
@@ -51,23 +53,23 @@ __global__ void __launch_bounds__(1024, 1) k_l2_gather(const float2 *__restrict_
 extern "C" int tb_bench_l2_gather(tb_ctx *ctx, long long bytes, double *gbs) {
     if (!ctx || !gbs || bytes < 4096 || bytes > (1LL << 30)) return TB_ERR_ARG;
     TB_CUDA(ctx, cudaSetDevice(ctx->device));
-    unsigned long long words = 1;
-    while (words * 2 * sizeof(float2) <= (unsigned long long)bytes) words *= 2;  // largest power of two that fits
-    const int threads = 1024, iters = 1 << 12;
+    unsigned long long sectors = 1;
+    while (sectors * 2 * 32 <= (unsigned long long)bytes) sectors *= 2;  // largest power of two that fits
+    const int threads = 1024, iters = 1 << 11;
     const int blocks = ctx->num_sms;
-    float2 *buf = nullptr;
+    float4 *buf = nullptr;
     float *sink = nullptr;
     cudaEvent_t a, b;
-    TB_CUDA(ctx, cudaMalloc(&buf, words * sizeof(float2)));
-    TB_CUDA(ctx, cudaMemset(buf, 0, words * sizeof(float2)));
+    TB_CUDA(ctx, cudaMalloc(&buf, sectors * 32));
+    TB_CUDA(ctx, cudaMemset(buf, 0, sectors * 32));
     TB_CUDA(ctx, cudaMalloc(&sink, blocks * sizeof(float)));
     TB_CUDA(ctx, cudaEventCreate(&a));
     TB_CUDA(ctx, cudaEventCreate(&b));
-    k_l2_gather<<<blocks, threads>>>(buf, (unsigned)(words - 1), iters, sink);  // warm-up: the buffer enters L2
+    k_l2_gather<<<blocks, threads>>>(buf, (unsigned)(sectors - 1), iters, sink);  // warm-up: the buffer enters L2
     TB_CUDA(ctx, cudaGetLastError());
     TB_CUDA(ctx, cudaDeviceSynchronize());
     TB_CUDA(ctx, cudaEventRecord(a));
-    k_l2_gather<<<blocks, threads>>>(buf, (unsigned)(words - 1), iters, sink);
+    k_l2_gather<<<blocks, threads>>>(buf, (unsigned)(sectors - 1), iters, sink);
     TB_CUDA(ctx, cudaGetLastError());
     TB_CUDA(ctx, cudaEventRecord(b));
     TB_CUDA(ctx, cudaEventSynchronize(b));
@@ -77,7 +79,7 @@ extern "C" int tb_bench_l2_gather(tb_ctx *ctx, long long bytes, double *gbs) {
     cudaEventDestroy(b);
     cudaFree(sink);
     cudaFree(buf);
-    *gbs = (double)blocks * threads * (double)iters * 4 * sizeof(float2) / (ms * 1e-3) / 1e9;
+    *gbs = (double)blocks * threads * (double)iters * 4 * 32 / (ms * 1e-3) / 1e9;
     return TB_OK;
 }
 
