@@ -16,7 +16,7 @@ def run(args, env=None):
 
 def test_reference_arm_prints_one_contract_line():
     import bench
-    r = run(["--impl", "reference", "--steps", "1", "--warmup", "3"])
+    r = run(["--impl", "reference", "--steps", "1", "--warmup", "3", "--particles", "8192"])
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
@@ -32,5 +32,6 @@ def test_reference_arm_prints_one_contract_line():
 
 
 def test_reference_arm_is_silent_on_other_ranks():
-    r = run(["--impl", "reference", "--steps", "1", "--warmup", "3"], env={"RANK": "1", "WORLD_SIZE": "2"})
+    r = run(["--impl", "reference", "--steps", "1", "--warmup", "3", "--particles", "8192"],
+            env={"RANK": "1", "WORLD_SIZE": "2"})
     assert r.returncode == 0 and not r.stdout.strip()
