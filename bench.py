@@ -1047,7 +1047,7 @@ def steady_measure(p):
 def adjoint_measure():
     """The adjoint on the AR-5 sensitivity workload (2^20 ions + 2^20 electrons per batch,
     50 batches, 64-bin IED, 32-bin IAD): recording time of the forward run (with 32
-    field-feedback modes every 5 batches), backward time of each objective, and the
+    field-feedback modes measured every batch), backward time of each objective, and the
     directional derivative along +-10% on the 140 eV peak's bins against central
     differences of the full charging chain on the same Philox draws."""
     import time
@@ -1066,7 +1066,7 @@ def adjoint_measure():
     vE = np.where(np.abs(cE - 140) < 15, 1.0, 0.0)
     out = {"workload": "AR-5 trench 20x100 cells (60x180 grid), floating conductive mask; 64-bin IED 0-300 eV, "
                        "32-bin IAD 0-10 deg; 2^20 ions + 2^20 electrons per batch; 50 batches; "
-                       "histories checkpointed every 10 batches; 32 feedback modes every 5 batches",
+                       "histories checkpointed every 10 batches; 32 feedback modes measured every batch",
            "record_s": record_s, "record_particles_per_s": 2 * p.n_per_batch * B / record_s}
     f64 = torch.float64
     for name in ("phi_bottom", "ratio_i_bottom"):

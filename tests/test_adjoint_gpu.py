@@ -263,7 +263,7 @@ def test_reverse_sweep_with_feedback_matches_the_fp64_torch_gradient(mods, recor
 
 def test_gradient_tracks_the_full_charging_chain(mods):
     """AR-5 workload at full size (2^20 ions + 2^20 electrons per batch, 50 batches):
-    directional derivatives of the adjoint (32 feedback modes every 5 batches)
+    directional derivatives of the adjoint (32 feedback modes measured every batch)
     against central differences of the full charging chain, each chain re-traced
     with the perturbed histograms on the same Philox draws (common random numbers),
     steps of +-10% on the 140 eV peak's bins and on the angle bins above 3 deg.
