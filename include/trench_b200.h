@@ -119,15 +119,12 @@ int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream
  * threads for batches of SMs x 768 particles and more, 128 at the least).  Chosen by the
  * autotuner (ChargingCase.autotune_tracer). */
 int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
-/* Order in which the FP32 tracer's lanes claim particles: 0 in index order (default),
- * 1 from the last index down, 2 learned: longest predicted first, the prediction being
- * the mean step count of the particle's bin (species, starting column band, direction
- * octant, kinetic energy band) in the previous trace on this context, so the launch does
- * not end waiting for long trajectories claimed last.  Results do not depend on the
- * order; the time does.  The learned order's buffers are allocated by the first trace
- * that uses it outside a stream capture (a capture before that traces in index order).
- * Chosen by the autotuner. */
-int tb_set_claim_order(tb_ctx *ctx, int order);
+/* Order in which the FP32 tracer's lanes claim particles: 0 in index order
+ * (default), 1 from the last index down.  Results do not depend on it; the time
+ * does, because the launch ends with the longest trajectories claimed last (in a
+ * batch of ions then electrons whose electrons run longest, reverse order drains
+ * sooner).  Chosen by the autotuner. */
+int tb_set_claim_order(tb_ctx *ctx, int reverse);
 
 /* Synchronise `stream`, then read and clear the context's device-side check flag:
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the

@@ -13,6 +13,7 @@ from conftest import load_golden
 from oracle import oracle_fields as OF
 from oracle import oracle_trace as OT
 from trench_b200 import geometry, inject
+from trench_b200.step import CLAIM_ORDERS
 from trench_b200.params import EPS0, Params
 
 pytestmark = pytest.mark.gpu
@@ -385,7 +386,7 @@ def test_autotuners_pick_a_shape_and_keep_results(case_cls):
     parts = inject.inject(p, p.n_per_batch, tuned.ny, np.random.default_rng(3))
     tuned.load(*parts)
     timings = tuned.autotune_tracer()
-    assert set(timings) == {(t, c, o) for t, c in tuned.TRACER_SHAPES for o in (0, 1)}
+    assert set(timings) == {(t, c, o) for t, c in tuned.TRACER_SHAPES for o in range(len(CLAIM_ORDERS))}
     counts, hits = [], []
     from trench_b200 import _capi
     tuned.hit = torch.full((tuned.capacity,), -1, dtype=torch.int32, device=tuned.dev)
@@ -400,8 +401,8 @@ def test_autotuners_pick_a_shape_and_keep_results(case_cls):
         np.testing.assert_array_equal(c, counts[0])
         np.testing.assert_array_equal(h, hits[0])
     assert "poisson_schedule" in tuned.tuning and "tracer_shape" in tuned.tuning
-    assert tuned.tuning["claim_order"] in ("index", "reverse")
-    assert _capi.lib().tb_set_claim_order(tuned.ctx.handle, 2) == _capi.TB_ERR_ARG
+    assert tuned.tuning["claim_order"] in CLAIM_ORDERS
+    assert _capi.lib().tb_set_claim_order(tuned.ctx.handle, len(CLAIM_ORDERS)) == _capi.TB_ERR_ARG
 
 
 class _StopAfter:

@@ -37,12 +37,6 @@ static int release(tb_ctx *c) {
     cudaFree(c->d_rf_barrier);
     cudaFree(c->d_queue);
     cudaFree(c->d_err);
-    cudaFree(c->d_order);
-    cudaFree(c->d_okey);
-    cudaFree(c->d_bin_sum);
-    cudaFree(c->d_bin_cnt);
-    cudaFree(c->d_bin_class);
-    cudaFree(c->d_class);
     tb_poisson_free(c->poisson);
     if (prev >= 0) cudaSetDevice(prev);
     delete c;

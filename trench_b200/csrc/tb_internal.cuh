@@ -99,13 +99,6 @@ __device__ __forceinline__ void tb_store_packed(tb_fcell *out, const uint8_t *va
 struct tb_poisson;
 void tb_poisson_free(tb_poisson *ps);
 
-// Learned claim order of the FP32 tracer: particles binned by species, starting column
-// (32 bands of the domain width), direction octant and kinetic energy (4 bands), each
-// bin's mean step count learned from the previous batch, bins grouped into classes of
-// decreasing predicted length.
-#define TB_ORDER_BINS 2048
-#define TB_ORDER_CLASSES 16
-
 struct tb_ctx {
     int device = 0;
     int nx = 0, ny = 0;
@@ -124,15 +117,7 @@ struct tb_ctx {
     int smem_per_sm = 0;                 // shared memory of one SM (bytes)
     int tune_threads = 0;                // FP32 tracer CTA size (tb_set_tuning), 0 = by batch size
     int tune_ctas_per_sm = 1;            // FP32 tracer CTAs per SM
-    int tune_reverse = 0;                // FP32 tracer claim order: 0 index, 1 last index down, 2 learned
-    // learned claim order (order 2): particles claimed by predicted length, longest first
-    int *d_order = nullptr;              // (order_cap) particle index of each claim rank
-    uint16_t *d_okey = nullptr;          // (order_cap) bin of each particle of the batch
-    int order_cap = 0;
-    unsigned long long *d_bin_sum = nullptr;  // (TB_ORDER_BINS) steps per bin of the last batch
-    unsigned *d_bin_cnt = nullptr;       // (TB_ORDER_BINS) particles per bin of the last batch
-    uint8_t *d_bin_class = nullptr;      // (TB_ORDER_BINS) claim class of each bin, 0 = longest
-    unsigned *d_class = nullptr;         // (3 x TB_ORDER_CLASSES) counts, offsets, fill levels
+    int tune_reverse = 0;                // FP32 tracer claims particles from the last index down
     float4 *d_rf_field = nullptr;        // circuit_rf basis fields (exs, eys, exm, eym) x vac, halo-padded
     float4 *d_rf_barrier = nullptr;      // (2, nx*ny) per-face wall barrier of each basis potential
     int rf_ready = 0;

@@ -44,7 +44,6 @@ struct K32 {
     int bytes;                      // packed field bytes (multiple of 16)
     int pool_off;                   // byte offset of the drain pool in dynamic shared memory, -1 = none
     int reverse;                    // claim particles from the last index down
-    const int *order;               // learned claim order: particle of each claim rank (nullptr = none)
     // circuit_rf in flight (kernels with RF = true): the unit-voltage basis fields
     // (exs, eys, exm, eym) x vac in field units per padded cell, their per-face wall
     // barriers (substrate basis then mask basis, nx*ny each), the waveform per table
@@ -483,11 +482,8 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                 if (s.pid < 0) {
                     // claim order: index order, or from the last index down (k.reverse)
                     const unsigned long long rank = base + __popc(need & ((1u << lane) - 1u));
-                    const bool in = rank < (unsigned long long)a.n;
                     const unsigned long long idx =
-                        !in ? rank
-                            : (k.order ? (unsigned long long)__ldg(k.order + rank)
-                                       : (k.reverse ? (unsigned long long)a.n - 1 - rank : rank));
+                        (k.reverse && rank < (unsigned long long)a.n) ? (unsigned long long)a.n - 1 - rank : rank;
                     if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
                         const int pid = (int)idx;
                         s.pid = pid;
@@ -704,139 +700,7 @@ __global__ void pack_rf_fields_kernel(int nx, int ny, double scale_e, double sca
     }
 }
 
-// ---- learned claim order ----------------------------------------------------------------
-// Bin of a particle: species, starting column band (32 across the domain), direction
-// octant and kinetic energy band (below 5, 20, 80 eV, above).
-__device__ __forceinline__ int order_bin(const tb_trace_args &a, long long i, double inv_lx) {
-    const double x = a.d_x[i], vx = a.d_vx[i], vy = a.d_vy[i], qm = a.d_qm[i];
-    const int spc = a.d_spc[i] ? 1 : 0;
-    const int xb = min(max((int)(x * inv_lx * 32.0), 0), 31);
-    const int oct = (vx >= 0 ? 4 : 0) | (vy >= 0 ? 2 : 0) | (fabs(vx) > fabs(vy) ? 1 : 0);
-    const double e = 0.5 * (vx * vx + vy * vy) / fmax(fabs(qm), 1e-300);  // kinetic energy, eV
-    const int eb = e < 5.0 ? 0 : (e < 20.0 ? 1 : (e < 80.0 ? 2 : 3));
-    return ((spc * 32 + xb) * 8 + oct) * 4 + eb;
-}
-
-// Bins of the batch and the particle count of each claim class.
-__global__ void k_order_bins(const tb_trace_args a, double inv_lx, uint16_t *key, const uint8_t *bin_class,
-                             unsigned *count) {
-    __shared__ unsigned h[TB_ORDER_CLASSES];
-    if (threadIdx.x < TB_ORDER_CLASSES) h[threadIdx.x] = 0;
-    __syncthreads();
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
-        const int b = order_bin(a, i, inv_lx);
-        key[i] = (uint16_t)b;
-        atomicAdd(&h[bin_class[b]], 1u);
-    }
-    __syncthreads();
-    if (threadIdx.x < TB_ORDER_CLASSES && h[threadIdx.x]) atomicAdd(&count[threadIdx.x], h[threadIdx.x]);
-}
-
-// Start of each class in the claim order; counts and fill levels cleared for the next use.
-__global__ void k_order_scan(unsigned *cls) {
-    if (threadIdx.x == 0) {
-        unsigned off = 0;
-        for (int c = 0; c < TB_ORDER_CLASSES; ++c) {
-            cls[TB_ORDER_CLASSES + c] = off;
-            off += cls[c];
-            cls[c] = 0;
-            cls[2 * TB_ORDER_CLASSES + c] = 0;
-        }
-    }
-}
-
-// Each particle's claim rank: its class's start plus its place in the class (lanes of a
-// warp in one class reserve their places with one atomic).
-__global__ void k_order_scatter(long long n, const uint16_t *key, const uint8_t *bin_class, unsigned *cls,
-                                int *order) {
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < n; i0 += (long long)gridDim.x * blockDim.x) {
-        const long long i = i0 + threadIdx.x;
-        const int c = i < n ? bin_class[key[i]] : TB_ORDER_CLASSES;
-        const unsigned peers = __match_any_sync(FULL, c);
-        const int leader = __ffs(peers) - 1;
-        unsigned base = 0;
-        if (lane == leader && c < TB_ORDER_CLASSES) base = atomicAdd(&cls[2 * TB_ORDER_CLASSES + c], __popc(peers));
-        base = __shfl_sync(FULL, base, leader);
-        if (c < TB_ORDER_CLASSES)
-            order[cls[TB_ORDER_CLASSES + c] + base + __popc(peers & ((1u << lane) - 1u))] = (int)i;
-    }
-}
-
-// After the trace: steps and particles per bin.
-__global__ void k_order_learn(long long n, const uint16_t *key, const int32_t *steps, unsigned long long *sum,
-                              unsigned *cnt) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const int b = key[i];
-        atomicAdd(&sum[b], (unsigned long long)steps[i]);
-        atomicAdd(&cnt[b], 1u);
-    }
-}
-
-// Class of each bin for the next batch from its mean steps (bins without particles take
-// the batch mean): class 0 for the longest mean, classes in equal steps of the longest
-// mean down to 15; the sums are cleared.
-__global__ void __launch_bounds__(1024) k_order_classes(unsigned long long *sum, unsigned *cnt, uint8_t *bin_class) {
-    __shared__ double sh_s[32], sh_c[32], sh_m[32];
-    double ts = 0, tc = 0;
-    for (int b = threadIdx.x; b < TB_ORDER_BINS; b += blockDim.x) { ts += (double)sum[b]; tc += (double)cnt[b]; }
-    for (int o = 16; o > 0; o >>= 1) { ts += __shfl_down_sync(0xffffffffu, ts, o); tc += __shfl_down_sync(0xffffffffu, tc, o); }
-    if ((threadIdx.x & 31) == 0) { sh_s[threadIdx.x >> 5] = ts; sh_c[threadIdx.x >> 5] = tc; }
-    __syncthreads();
-    ts = tc = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { ts += sh_s[w]; tc += sh_c[w]; }
-    const double mean = tc > 0 ? ts / tc : 0.0;
-    double mx = 0;
-    for (int b = threadIdx.x; b < TB_ORDER_BINS; b += blockDim.x)
-        mx = fmax(mx, cnt[b] ? (double)sum[b] / cnt[b] : mean);
-    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) sh_m[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    mx = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, sh_m[w]);
-    for (int b = threadIdx.x; b < TB_ORDER_BINS; b += blockDim.x) {
-        const double m = cnt[b] ? (double)sum[b] / cnt[b] : mean;
-        const int c = mx > 0 ? (int)(TB_ORDER_CLASSES * (1.0 - m / (mx * 1.000001))) : 0;
-        bin_class[b] = (uint8_t)min(max(c, 0), TB_ORDER_CLASSES - 1);
-        sum[b] = 0;
-        cnt[b] = 0;
-    }
-}
-
 }  // namespace
-
-// Buffers of the learned claim order for n particles; false (order left off) when they
-// would need an allocation during a stream capture or the allocation fails.
-static bool order_buffers(tb_ctx *ctx, long long n, cudaStream_t s) {
-    if (ctx->d_bin_sum && n <= ctx->order_cap) return true;
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return false;
-    if (!ctx->d_bin_sum) {
-        if (cudaMalloc(&ctx->d_bin_sum, TB_ORDER_BINS * sizeof(unsigned long long)) != cudaSuccess ||
-            cudaMalloc(&ctx->d_bin_cnt, TB_ORDER_BINS * sizeof(unsigned)) != cudaSuccess ||
-            cudaMalloc(&ctx->d_bin_class, TB_ORDER_BINS) != cudaSuccess ||
-            cudaMalloc(&ctx->d_class, 3 * TB_ORDER_CLASSES * sizeof(unsigned)) != cudaSuccess)
-            return false;
-        cudaMemset(ctx->d_bin_sum, 0, TB_ORDER_BINS * sizeof(unsigned long long));
-        cudaMemset(ctx->d_bin_cnt, 0, TB_ORDER_BINS * sizeof(unsigned));
-        cudaMemset(ctx->d_bin_class, 0, TB_ORDER_BINS);
-        cudaMemset(ctx->d_class, 0, 3 * TB_ORDER_CLASSES * sizeof(unsigned));
-    }
-    if (n > ctx->order_cap) {
-        cudaFree(ctx->d_order);
-        cudaFree(ctx->d_okey);
-        ctx->d_order = nullptr;
-        ctx->d_okey = nullptr;
-        ctx->order_cap = 0;
-        if (cudaMalloc(&ctx->d_order, n * sizeof(int)) != cudaSuccess ||
-            cudaMalloc(&ctx->d_okey, n * sizeof(uint16_t)) != cudaSuccess)
-            return false;
-        ctx->order_cap = (int)n;
-    }
-    cudaGetLastError();
-    return true;
-}
 
 int tb_launch_pack_rf_fields(tb_ctx *ctx, const double *rf_ex, const double *rf_ey, const double *rf_phi,
                              const double *wface, const double *wave, int n_phase, cudaStream_t s) {
@@ -912,8 +776,7 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.err = ctx->d_err;
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     k.pool_off = -1;
-    k.reverse = ctx->tune_reverse == 1;
-    k.order = nullptr;
+    k.reverse = ctx->tune_reverse;
     k.rf_field = ctx->d_rf_field;
     k.rf_barrier = ctx->d_rf_barrier;
     k.rf_wave = ctx->d_rf_wave;
@@ -942,17 +805,6 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     K32 k = make_k32(ctx, a);
     const bool rf = a->n_phase > 0;
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
-    // learned claim order: particles claimed longest predicted first, so the launch does
-    // not end waiting for long trajectories claimed last
-    const bool learned = ctx->tune_reverse == 2 && a->n <= 0x7fffffffLL && order_buffers(ctx, a->n, s);
-    const int oblocks = (int)std::min<long long>((a->n + 255) / 256, 4LL * std::max(ctx->num_sms, 1));
-    if (learned) {
-        const double inv_lx = 1.0 / (ctx->nx * ctx->dx);
-        k_order_bins<<<oblocks, 256, 0, s>>>(*a, inv_lx, ctx->d_okey, ctx->d_bin_class, ctx->d_class);
-        k_order_scan<<<1, 32, 0, s>>>(ctx->d_class);
-        k_order_scatter<<<oblocks, 256, 0, s>>>(a->n, ctx->d_okey, ctx->d_bin_class, ctx->d_class, ctx->d_order);
-        k.order = ctx->d_order;
-    }
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
     int threads = ctx->tune_threads;
@@ -993,10 +845,6 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     else if (threads == 768) TB_LAUNCH_F32(768);
     else TB_LAUNCH_F32(1024);
 #undef TB_LAUNCH_F32
-    if (learned) {
-        k_order_learn<<<oblocks, 256, 0, s>>>(a->n, ctx->d_okey, a->d_steps, ctx->d_bin_sum, ctx->d_bin_cnt);
-        k_order_classes<<<1, 1024, 0, s>>>(ctx->d_bin_sum, ctx->d_bin_cnt, ctx->d_bin_class);
-    }
     TB_CUDA(ctx, cudaGetLastError());
     return TB_OK;
 }
@@ -1295,10 +1143,10 @@ extern "C" int tb_pack_check(tb_pack *p, void *stream) {
 }
 
 
-extern "C" int tb_set_claim_order(tb_ctx *ctx, int order) {
+extern "C" int tb_set_claim_order(tb_ctx *ctx, int reverse) {
     if (!ctx) return TB_ERR_ARG;
-    if (order < 0 || order > 2) return tb_fail(ctx, TB_ERR_ARG, "tb_set_claim_order: order must be 0, 1 or 2");
-    ctx->tune_reverse = order;
+    if (reverse != 0 && reverse != 1) return tb_fail(ctx, TB_ERR_ARG, "tb_set_claim_order: order must be 0 or 1");
+    ctx->tune_reverse = reverse;
     return TB_OK;
 }
 
