@@ -375,6 +375,10 @@ int tb_bench_smem(tb_ctx *ctx, double *gbs);
  * stays in L2, like the FP32 tracer's field on grids too large for shared memory.  Allocates and frees
  * its buffer; synchronises the device. */
 int tb_bench_l2_gather(tb_ctx *ctx, long long bytes, double *gbs);
+/* Self-check of the FP64 tracer's quotients by a divisor with a known reciprocal (cell
+ * size, RF period): on n seeded pairs of each of three input families, counts the
+ * quotients that differ in any bit from the IEEE division.  Synchronises the device. */
+int tb_check_div_by(tb_ctx *ctx, long long n, unsigned long long seed, unsigned long long *mismatches);
 
 #ifdef __cplusplus
 }

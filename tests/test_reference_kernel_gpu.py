@@ -136,7 +136,9 @@ def test_circuit_rf_batch_against_the_reference_kernel(cuda_device):
     """One batch of the reference's circuit_rf benchmark run (120 x 560 grid, pulsed 5 kV,
     3000 ions + 3000 electrons at stratified phases): the reference kernel driven like the
     reference and the B200 FP64 kernel give the same counts; the B200 FP32 kernel agrees on
-    >= 99.9 % of the particles' outcomes and is faster than the reference kernel."""
+    >= 99.9 % of the particles' outcomes; both B200 kernels are faster than the reference
+    kernel (a batch this small is bound by the step latency of its longest trajectories,
+    not by throughput)."""
     import torch
     import bench
     from trench_b200 import geometry, inject
@@ -175,3 +177,4 @@ def test_circuit_rf_batch_against_the_reference_kernel(cuda_device):
             json.dump(report, fh, indent=1)
     assert same.mean() >= 0.999
     assert t_f32 < t_ref
+    assert t_f64 < t_ref

@@ -256,6 +256,20 @@ def test_chunked_run_with_stop_equals_single_launch(tracers):
         np.testing.assert_array_equal(u, v)
 
 
+def test_f64_quotients_by_a_known_reciprocal_equal_the_division(cuda_device):
+    """The FP64 tracer divides by the cell size and the RF period through the rounded
+    reciprocal and one exact correction; on 2^26 seeded pairs of each of three families
+    (wide exponents, the tracer's positions over cell sizes, divisors near the ends of a
+    binade) every quotient equals the IEEE division bit for bit."""
+    import ctypes
+    from trench_b200 import _capi
+    from trench_b200.tracer import Context
+    ctx = Context(np.ones((4, 4), bool), cuda_device)
+    bad = ctypes.c_ulonglong(1)
+    ctx.check(_capi.lib().tb_check_div_by(ctx.handle, 1 << 26, 77, ctypes.byref(bad)))
+    assert bad.value == 0
+
+
 def test_invalid_device_is_reported(cuda_device):
     from trench_b200.tracer import B200Tracer
     with pytest.raises(RuntimeError, match="デバイス"):

@@ -143,6 +143,7 @@ SIGNATURES = {
     "tb_step_monitors": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp, _vp, ctypes.c_int, _vp, _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
     "tb_bench_l2_gather": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.POINTER(_dbl)]),
+    "tb_check_div_by": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong)]),
     "tb_inject": (ctypes.c_int, [_vp, ctypes.POINTER(InjectArgs), _vp]),
     "tb_philox_fill": (ctypes.c_int, [_vp, ctypes.c_ulonglong, ctypes.c_ulonglong, ctypes.c_int, _vp, _vp]),
     "tb_pack_create": (ctypes.c_int, [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)]),

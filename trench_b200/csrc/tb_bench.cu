@@ -48,7 +48,62 @@ __global__ void __launch_bounds__(1024, 1) k_l2_gather(const float4 *__restrict_
     if (acc == -1.f) sink[blockIdx.x] = acc;  // keeps the loads live
 }
 
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+
+// tb_div_by(a, b, RN(1/b)) against a / b on n seeded pairs of one family: 0 any
+// significands with exponents within +-60, 1 positions 0-10 um over cell sizes
+// 0.1-10 nm, 2 divisors with significands near all-ones or near one.
+__global__ void k_check_div_by(long long n, unsigned long long seed, int family, unsigned long long *bad) {
+    unsigned long long mine = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint64_t h1 = mix64(2 * (uint64_t)i + seed * 0x9E3779B97F4A7C15ULL);
+        const uint64_t h2 = mix64(2 * (uint64_t)i + 1 + seed * 0x9E3779B97F4A7C15ULL);
+        double a, b;
+        if (family == 0) {
+            a = __longlong_as_double((long long)((h1 & 0x000fffffffffffffULL) | ((uint64_t)(1023 - 60 + (h1 >> 52) % 121) << 52)));
+            b = __longlong_as_double((long long)((h2 & 0x000fffffffffffffULL) | ((uint64_t)(1023 - 60 + (h2 >> 52) % 121) << 52)));
+            if (h1 >> 63) a = -a;
+        } else if (family == 1) {
+            b = 1e-10 * (1.0 + 99.0 * (double)(h2 >> 11) * 0x1p-53);
+            a = 1e-5 * ((double)(h1 >> 11) * 0x1p-53 - 0.01);
+        } else {
+            const uint64_t m = (h2 & 1) ? (0x000fffffffffffffULL - (h2 >> 40)) : (h2 >> 40);
+            b = __longlong_as_double((long long)(m | (1023ULL << 52)));
+            a = __longlong_as_double((long long)((h1 & 0x000fffffffffffffULL) | ((uint64_t)(1023 - 5 + (h1 >> 52) % 11) << 52)));
+        }
+        const double q0 = a / b, q1 = tb_div_by(a, b, 1.0 / b);
+        mine += __double_as_longlong(q0) != __double_as_longlong(q1);
+    }
+    for (int o = 16; o > 0; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(bad, mine);
+}
+
 }  // namespace
+
+extern "C" int tb_check_div_by(tb_ctx *ctx, long long n, unsigned long long seed, unsigned long long *mismatches) {
+    if (!ctx || !mismatches || n < 0) return TB_ERR_ARG;
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    unsigned long long *bad = nullptr;
+    TB_CUDA(ctx, cudaMalloc(&bad, sizeof(unsigned long long)));
+    TB_CUDA(ctx, cudaMemset(bad, 0, sizeof(unsigned long long)));
+    for (int family = 0; family < 3; ++family)
+        k_check_div_by<<<ctx->num_sms * 8, 256>>>(n, seed + (unsigned long long)family, family, bad);
+    const cudaError_t e = cudaGetLastError();
+    unsigned long long h = 0;
+    const cudaError_t c = cudaMemcpy(&h, bad, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(bad);
+    TB_CUDA(ctx, e);
+    TB_CUDA(ctx, c);
+    *mismatches = h;
+    return TB_OK;
+}
 
 extern "C" int tb_bench_l2_gather(tb_ctx *ctx, long long bytes, double *gbs) {
     if (!ctx || !gbs || bytes < 4096 || bytes > (1LL << 30)) return TB_ERR_ARG;

@@ -180,6 +180,19 @@ __device__ __forceinline__ void tb_deposit(int32_t *counts, size_t key) {
     if ((int)(threadIdx.x & 31u) == __ffs(peers) - 1) atomicAdd(counts + key, __popc(peers));
 }
 
+// a / b rounded to nearest for a divisor b whose rounded reciprocal rb = RN(1/b) is known:
+// q = RN(a rb) is within one ulp of a/b, and one correction with the exact remainder
+// a - b q (a fused multiply-add) gives the correctly rounded quotient (Markstein's
+// theorem: P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990).  Three dependent operations in place of a full
+// division; valid while no intermediate overflows or underflows.  tb_check_div_by compares
+// it with the division on the device.
+__device__ __forceinline__ double tb_div_by(double a, double b, double rb) {
+    const double q = __dmul_rn(a, rb);
+    const double r = fma(-q, b, a);
+    return fma(r, rb, q);
+}
+
 // Periodic index helpers.
 __host__ __device__ __forceinline__ int tb_wrap(int i, int n) {
     return i < 0 ? i + n : (i >= n ? i - n : i);

@@ -17,6 +17,10 @@
 //  * Persistent warps, one particle per lane, lanes refill from a global atomic
 //    queue as soon as their particle ends (no lane waits for a slow electron).
 //  * Absorbed particles are deposited with integer atomics (bit-exact counts).
+//  * The x/y-symmetric arithmetic of a step (half-cell shift, the bilinear sums of
+//    (Ex, Ey), acceleration, velocity and position updates, cell remainder) runs on
+//    packed FP32 pairs (sm_100 f32x2 add/mul/fma): one instruction per pair, which
+//    cuts the issued instructions of this issue-bound loop by about an eighth.
 // The step follows the reference algorithm (trench_charging_2d.py:584-650,
 // trench_trace.cu:92-148): vacuum-weighted bilinear field, CFL step, trapezoid
 // update, periodic x, escape at the top, staircase corner crossing, first-face
@@ -120,7 +124,8 @@ __device__ bool stage_field(void *dst, const void *src, int bytes, uint64_t *mba
 // velocity in vscale units; pid < 0 = no particle.
 struct LaneState {
     int pid, ix, iy, steps, stop_at, spc;
-    float ox, oy, vx, vy, qm;
+    float2 o, v;                    // offset (ox, oy) and velocity (vx, vy), packed pairs
+    float qm;
     uint32_t clock;                 // circuit_rf: clock in 2^-32 of the period
     float elapsed;                  // circuit_rf: seconds in flight
 };
@@ -178,9 +183,9 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     // ---- vacuum-weighted bilinear field (trench_charging_2d.py:492-509) ----
     // corners (i0, j0) = (ix - 1 + hx, iy - 1 + hy) .. (i0 + 1, j0 + 1); in the halo-padded
     // field i0 + 1 = ix + hx needs no wrap and the clipped rows need one clamp
-    const int hx = s.ox >= 0.5f ? 1 : 0, hy = s.oy >= 0.5f ? 1 : 0;
-    const float tx = hx ? s.ox - 0.5f : s.ox + 0.5f;
-    const float ty = hy ? s.oy - 0.5f : s.oy + 0.5f;
+    const int hx = s.o.x >= 0.5f ? 1 : 0, hy = s.o.y >= 0.5f ? 1 : 0;
+    const float2 tq = __fadd2_rn(s.o, make_float2(hx ? -0.5f : 0.5f, hy ? -0.5f : 0.5f));
+    const float tx = tq.x, ty = tq.y;
     const int base = (s.ix + hx) * P + max(s.iy + hy, 0);
     tb_fcell c00, c01, c10, c11;
     if (SMEM) {
@@ -200,24 +205,33 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     // four are vacuum: then the step cannot reach a wall and the vacuum weights sum to one,
     // and both the normalisation and the end-cell checks are skipped.
     const bool near = !(C.small_steps && (__float_as_uint(c00.ey) & 1u));
-    const float ux = 1.f - tx, uy = 1.f - ty;
-    const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
-    const float sex = w00 * c00.ex + w10 * c10.ex + w01 * c01.ex + w11 * c11.ex;
-    const float sey = w00 * c00.ey + w10 * c10.ey + w01 * c01.ey + w11 * c11.ey;
+    // bilinear sum of the (vacuum-premultiplied) field with (ex, ey) as one packed pair:
+    // along y in both columns, then along x
+    const float2 M1 = make_float2(-1.f, -1.f);
+    const float2 tyy = make_float2(ty, ty), txx = make_float2(tx, tx);
+    const float2 f00 = make_float2(c00.ex, c00.ey), f01 = make_float2(c01.ex, c01.ey);
+    const float2 f10 = make_float2(c10.ex, c10.ey), f11 = make_float2(c11.ex, c11.ey);
+    const float2 e0 = __ffma2_rn(tyy, __ffma2_rn(f00, M1, f01), f00);
+    const float2 e1 = __ffma2_rn(tyy, __ffma2_rn(f10, M1, f11), f10);
+    const float2 E = __ffma2_rn(txx, __ffma2_rn(e0, M1, e1), e0);
+    const float sex = E.x, sey = E.y;
     float inv_sw = 1.f;
     if (near) {
-        const float sw = w00 * vac_of(c00) + w10 * vac_of(c10) + w01 * vac_of(c01) + w11 * vac_of(c11);
-        inv_sw = __fdividef(1.f, fmaxf(sw, 1e-12f));
+        const float v00 = vac_of(c00), v01 = vac_of(c01), v10 = vac_of(c10), v11 = vac_of(c11);
+        const float s0 = fmaf(ty, v01 - v00, v00), s1 = fmaf(ty, v11 - v10, v10);
+        inv_sw = __fdividef(1.f, fmaxf(fmaf(tx, s1 - s0, s0), 1e-12f));
     }
-    float ax, ay, dt;
-    const float speed = sqrtf(s.vx * s.vx + s.vy * s.vy);
+    float2 A;
+    float dt;
+    const float speed = sqrtf(fmaf(s.v.x, s.v.x, s.v.y * s.v.y));
     if (!RF) {
         const float qs = s.qm * inv_sw;
-        ax = qs * sex;
-        ay = qs * sey;
-        const float acc = sqrtf(ax * ax + ay * ay);
+        A = __fmul2_rn(make_float2(qs, qs), E);
+        const float acc = sqrtf(fmaf(A.x, A.x, A.y * A.y));
         dt = __fdividef(C.cfl, speed + sqrtf(2.f * acc) + C.inv_v);
     } else {
+        const float ux = 1.f - tx, uy = 1.f - ty;
+        const float w00 = ux * uy, w10 = tx * uy, w01 = ux * ty, w11 = tx * ty;
         // in-flight RF field (trench_trace.cu:97-110): the basis fields at the same corners
         // and weights bound the step, and the field is taken at the mid-step clock.  The
         // waveform interval of the start clock is loaded before the step is known: a
@@ -245,22 +259,26 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         const float4 e = im == i0 ? e0 : __ldg(k.rf_wave + im);
         const float vs = fmaf(w, e.z, e.x), vm = fmaf(w, e.w, e.y);
         const float qs = s.qm * inv_sw;
-        ax = qs * (sex + (vs * sxs + vm * sxm));
-        ay = qs * (sey + (vs * sys + vm * sym));
+        A = make_float2(qs * (sex + (vs * sxs + vm * sxm)), qs * (sey + (vs * sys + vm * sym)));
         s.clock = c0 + (uint32_t)inc;
         s.elapsed += dt * k.t_sec;
     }
 
     // ---- CFL step and trapezoid update (trench_charging_2d.py:587-608) ----
-    const float vxn = s.vx + ax * dt, vyn = s.vy + ay * dt;
-    const float sx = 0.5f * (s.vx + vxn) * dt, sy = 0.5f * (s.vy + vyn) * dt;
-    // a step moves less than one cell, so the new offset lies in (-1, 2): the cell
-    // change is its floor (-1, 0 or 1) and the new offset the remainder (exact for the
-    // shift by 1; a remainder that rounds up to 1 is clamped below 1)
-    const float fnx = floorf(s.ox + sx), fny = floorf(s.oy + sy);
+    // v' = v + a dt and the move (v + v') dt / 2 = (v + a dt / 2) dt, each a packed pair.
+    // A step moves less than one cell, so the new offset lies in (-1, 2): the cell change
+    // is its floor (-1, 0 or 1) and the new offset the remainder (exact for the shift by
+    // 1; a remainder that rounds up to 1 is clamped below 1)
+    const float2 dtt = make_float2(dt, dt);
+    const float hdt = 0.5f * dt;
+    const float2 vn = __ffma2_rn(A, dtt, s.v);
+    const float2 S = __fmul2_rn(__ffma2_rn(A, make_float2(hdt, hdt), s.v), dtt);
+    const float vxn = vn.x, vyn = vn.y, sx = S.x, sy = S.y;
+    const float2 pos = __fadd2_rn(s.o, S);
+    const float fnx = floorf(pos.x), fny = floorf(pos.y);
     const int dix = (int)fnx, diy = (int)fny;
-    const float nox = fminf((s.ox + sx) - fnx, ONE_BELOW);
-    const float noy = fminf((s.oy + sy) - fny, ONE_BELOW);
+    const float2 rem = __ffma2_rn(make_float2(fnx, fny), M1, pos);
+    const float nox = fminf(rem.x, ONE_BELOW), noy = fminf(rem.y, ONE_BELOW);
     int nix = s.ix + dix;
     nix = nix < 0 ? nx - 1 : (nix >= nx ? 0 : nix);
     const int niy = s.iy + diy;
@@ -278,15 +296,15 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         if (corner) {
             const int y0c = min(max(s.iy, 0), ny - 1);
             const int iyn = min(max(niy, 0), ny - 1);
-            const float fx = ((dix > 0 ? 1.f : 0.f) - s.ox) / sx;
-            const float fy = ((iyn > y0c ? 1.f : 0.f) - s.oy) / sy;
+            const float fx = ((dix > 0 ? 1.f : 0.f) - s.o.x) / sx;
+            const float fy = ((iyn > y0c ? 1.f : 0.f) - s.o.y) / sy;
             const bool x_first = fx < fy;
             corner = !C.F.vac((x_first ? nix + 1 : s.ix + 1) * P + (x_first ? y0c : iyn) + 1);
         }
     }
 
     if (!(hit_end || corner || escaped || s.steps >= s.stop_at)) {
-        s.ix = nix; s.iy = niy; s.ox = nox; s.oy = noy; s.vx = vxn; s.vy = vyn;
+        s.ix = nix; s.iy = niy; s.o = make_float2(nox, noy); s.v = vn;
         return;
     }
 
@@ -300,8 +318,8 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
     if (hit ? C.first_face : corner) {
         // first solid face crossed (trench_charging_2d.py:512-539) in cell units
         const float inf = __int_as_float(0x7f800000);
-        const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - s.ox) / sx : inf;
-        const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - s.oy) / sy : inf;
+        const float fx = dix != 0 ? ((dix > 0 ? 1.f : 0.f) - s.o.x) / sx : inf;
+        const float fy = diy_e != 0 ? ((diy_e > 0 ? 1.f : 0.f) - s.o.y) / sy : inf;
         const bool x_first = fx < fy;
         const int ax_ = x_first ? nix : s.ix, ay_ = x_first ? y0c : y0c + diy_e;
         const bool use_last = dix != 0 && diy_e != 0 && C.F.vac((ax_ + 1) * P + ay_ + 1);
@@ -327,14 +345,14 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
             const float vn = face_x ? vxn : vyn;
             if (0.5f * vn * vn < s.qm * dphi) {
                 // reflect: the normal velocity flips, the position stays at the start point
-                s.vx = face_x ? -vxn : vxn;
-                s.vy = face_x ? vyn : -vyn;
+                s.v.x = face_x ? -vxn : vxn;
+                s.v.y = face_x ? vyn : -vyn;
                 hit = false;
                 reflected = true;
             }
         }
     }
-    if (!reflected) { s.ix = nix; s.iy = niy; s.ox = nox; s.oy = noy; s.vx = vxn; s.vy = vyn; }
+    if (!reflected) { s.ix = nix; s.iy = niy; s.o = make_float2(nox, noy); s.v = vn; }
 
     int done = 0;
     if (hit) {
@@ -359,10 +377,10 @@ __device__ __forceinline__ void step_particle(const K32 &k, const CaseView<SMEM>
         a.d_steps[pid] = s.steps;
         if (done != 3) a.d_status[pid] = (int8_t)done;
         if (done == 3 || a.write_state) {
-            a.d_x[pid] = ((double)s.ix + (double)s.ox) * k.dx;
-            a.d_y[pid] = ((double)s.iy + (double)s.oy) * k.dx;
-            a.d_vx[pid] = (double)s.vx * k.vscale;
-            a.d_vy[pid] = (double)s.vy * k.vscale;
+            a.d_x[pid] = ((double)s.ix + (double)s.o.x) * k.dx;
+            a.d_y[pid] = ((double)s.iy + (double)s.o.y) * k.dx;
+            a.d_vx[pid] = (double)s.v.x * k.vscale;
+            a.d_vy[pid] = (double)s.v.y * k.vscale;
         }
         if (RF) {
             a.d_clock[2 * pid] = (double)s.clock * 0x1p-32 * a.period;
@@ -388,10 +406,10 @@ __device__ __forceinline__ void pool_put(uint32_t *P, int T, int q, const LaneSt
     P[1 * T + q] = ((uint32_t)s.ix & 0xffffu) | ((uint32_t)s.iy << 16);
     P[2 * T + q] = (uint32_t)s.steps;
     P[3 * T + q] = (uint32_t)s.stop_at | ((uint32_t)s.spc << 31);
-    P[4 * T + q] = __float_as_uint(s.ox);
-    P[5 * T + q] = __float_as_uint(s.oy);
-    P[6 * T + q] = __float_as_uint(s.vx);
-    P[7 * T + q] = __float_as_uint(s.vy);
+    P[4 * T + q] = __float_as_uint(s.o.x);
+    P[5 * T + q] = __float_as_uint(s.o.y);
+    P[6 * T + q] = __float_as_uint(s.v.x);
+    P[7 * T + q] = __float_as_uint(s.v.y);
     P[8 * T + q] = __float_as_uint(s.qm);
     if (RF) {
         P[9 * T + q] = s.clock;
@@ -409,10 +427,10 @@ __device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneSt
     const uint32_t w = P[3 * T + q];
     s.stop_at = (int)(w & 0x7fffffffu);
     s.spc = (int)(w >> 31);
-    s.ox = __uint_as_float(P[4 * T + q]);
-    s.oy = __uint_as_float(P[5 * T + q]);
-    s.vx = __uint_as_float(P[6 * T + q]);
-    s.vy = __uint_as_float(P[7 * T + q]);
+    s.o.x = __uint_as_float(P[4 * T + q]);
+    s.o.y = __uint_as_float(P[5 * T + q]);
+    s.v.x = __uint_as_float(P[6 * T + q]);
+    s.v.y = __uint_as_float(P[7 * T + q]);
     s.qm = __uint_as_float(P[8 * T + q]);
     if (RF) {
         s.clock = P[9 * T + q];
@@ -456,7 +474,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     LaneState s;
     s.pid = -1;
     s.ix = s.iy = s.steps = s.stop_at = s.spc = 0;
-    s.ox = s.oy = s.vx = s.vy = s.qm = 0.f;
+    s.o.x = s.o.y = s.v.x = s.v.y = s.qm = 0.f;
     s.clock = 0u;
     s.elapsed = 0.f;
     LaneTally t = {0u, 0u, 0u, 0u, 0u, 0u};
@@ -493,10 +511,10 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                         const double xc = a.d_x[pid] * k.inv_dx, yc = a.d_y[pid] * k.inv_dx;
                         s.ix = min(max((int)xc, 0), C.nx - 1);
                         s.iy = min((int)floor(yc), C.ny - 1);  // a start above the grid escapes at once
-                        s.ox = fminf(fmaxf((float)(xc - (double)s.ix), 0.f), ONE_BELOW);
-                        s.oy = fminf(fmaxf((float)(yc - (double)s.iy), 0.f), ONE_BELOW);
-                        s.vx = (float)(a.d_vx[pid] * k.inv_v64);
-                        s.vy = (float)(a.d_vy[pid] * k.inv_v64);
+                        s.o.x = fminf(fmaxf((float)(xc - (double)s.ix), 0.f), ONE_BELOW);
+                        s.o.y = fminf(fmaxf((float)(yc - (double)s.iy), 0.f), ONE_BELOW);
+                        s.v.x = (float)(a.d_vx[pid] * k.inv_v64);
+                        s.v.y = (float)(a.d_vy[pid] * k.inv_v64);
                         s.qm = (float)a.d_qm[pid];
                         s.spc = a.d_spc[pid];
                         s.steps = a.d_steps[pid];

@@ -8,7 +8,11 @@
 // particle ends, so no lane idles behind a long electron trajectory and there is
 // no host round trip per 256-step chunk (trench_cuda.py:100-117).  Hits are
 // deposited on the device with integer atomics instead of a host bincount
-// (trench_cuda.py:118-121), so counts are exact and order-independent.
+// (trench_cuda.py:118-121), so counts are exact and order-independent.  Quotients by
+// the cell size and by the RF period, which sit on the step's dependency chain, come
+// from the rounded reciprocal and one exact correction (tb_div_by): the same quotient
+// as the division in three dependent operations, which is what bounds a small batch of
+// long trajectories.
 #include "tb_internal.cuh"
 
 namespace {
@@ -17,6 +21,7 @@ struct K64 {
     tb_trace_args a;
     int nx, ny;
     double dx;
+    double rdx, rperiod;            // RN(1/dx), RN(1/period): quotients by tb_div_by, exact
     const uint8_t *vac;
     unsigned long long *queue;
     int *err;
@@ -64,7 +69,7 @@ __device__ __forceinline__ int pmodll(int i, int n) {
 __device__ __forceinline__ void interp(const K64 &k, const double *ex, const double *ey, double x, double y,
                                        double &ox, double &oy) {
     const int nx = k.nx, ny = k.ny;
-    double fx = x / k.dx - 0.5, fy = y / k.dx - 0.5;
+    double fx = tb_div_by(x, k.dx, k.rdx) - 0.5, fy = tb_div_by(y, k.dx, k.rdx) - 0.5;
     int i0 = (int)floor(fx), j0 = (int)floor(fy);
     double tx = fx - (double)i0, ty = fy - (double)j0;
     int i1 = pmodll(i0 + 1, nx);
@@ -95,12 +100,12 @@ __device__ __forceinline__ void wall_entry(const K64 &k, double x0, double y0, d
                                            bool &face_x) {
     const int nx = k.nx, ny = k.ny;
     const double dx = k.dx;
-    int ix0 = (int)(x0 / dx);
+    int ix0 = (int)tb_div_by(x0, dx, k.rdx);
     if (ix0 > nx - 1) ix0 = nx - 1;
-    const int iy0 = clipll((int)(y0 / dx), ny);
+    const int iy0 = clipll((int)tb_div_by(y0, dx, k.rdx), ny);
     const double xu = x0 + sx, yu = y0 + sy;
-    const int dix = (int)floor(xu / dx) - ix0;
-    const int diy = clipll((int)floor(yu / dx), ny) - iy0;
+    const int dix = (int)floor(tb_div_by(xu, dx, k.rdx)) - ix0;
+    const int diy = clipll((int)floor(tb_div_by(yu, dx, k.rdx)), ny) - iy0;
     const double inf = __longlong_as_double(0x7ff0000000000000LL);
     const double fx = dix != 0 ? ((double)(ix0 + (dix > 0)) * dx - x0) / sx : inf;
     const double fy = diy != 0 ? ((double)(iy0 + (diy > 0)) * dx - y0) / sy : inf;
@@ -117,7 +122,7 @@ __device__ __forceinline__ void wall_entry(const K64 &k, double x0, double y0, d
 
 // Periodic linear interpolation of the electrode voltage deltas (trench_rf.py:5-11).
 __device__ __forceinline__ void rf_coeff(const K64 &k, double at, double &vs, double &vm) {
-    const double f = pymod(at, k.a.period) / k.a.period * (double)k.a.n_phase;
+    const double f = tb_div_by(pymod(at, k.a.period), k.a.period, k.rperiod) * (double)k.a.n_phase;
     const int i = pmodll((int)floor(f), k.a.n_phase);
     const int j = pmodll(i + 1, k.a.n_phase);
     const double w = f - floor(f);
@@ -177,16 +182,16 @@ __global__ void __launch_bounds__(256) trace_f64_kernel(const __grid_constant__ 
         ++my_steps;
 
         const bool escaped = y >= Ly;
-        int ix = (int)(x / dx);
+        int ix = (int)tb_div_by(x, dx, k.rdx);
         if (ix > nx - 1) ix = nx - 1;
-        int iy = clipll((int)(y / dx), ny);
+        int iy = clipll((int)tb_div_by(y, dx, k.rdx), ny);
         bool hit = !escaped && !__ldg(k.vac + ix * ny + iy);
         int cx = 0, cy = 0, vcx = 0, vcy = 0;
         bool face_x = false;
         if (a.tapered && !hit && !escaped) {
-            int ix0 = (int)(x0 / dx);
+            int ix0 = (int)tb_div_by(x0, dx, k.rdx);
             if (ix0 > nx - 1) ix0 = nx - 1;
-            const int iy0 = clipll((int)(y0 / dx), ny);
+            const int iy0 = clipll((int)tb_div_by(y0, dx, k.rdx), ny);
             if (ix != ix0 && iy != iy0) {
                 wall_entry(k, x0, y0, sx, sy, cx, cy, vcx, vcy, face_x);
                 hit = !__ldg(k.vac + cx * ny + cy);
@@ -356,6 +361,8 @@ int tb_launch_trace_f64(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     k.nx = ctx->nx;
     k.ny = ctx->ny;
     k.dx = ctx->dx;
+    k.rdx = 1.0 / ctx->dx;
+    k.rperiod = a->n_phase > 0 ? 1.0 / a->period : 0.0;
     k.vac = ctx->d_vac;
     k.queue = ctx->d_queue;
     k.err = ctx->d_err;
