@@ -372,6 +372,16 @@ def test_host_pipeline_equals_sequential_batches(case_cls):
     np.testing.assert_array_equal(a.rho(), b.rho())
     np.testing.assert_array_equal(rows.numpy(), b.hist[:4].cpu().numpy())
     np.testing.assert_array_equal(a.history()["ratio_e_bottom"], b.history()["ratio_e_bottom"])
+    # batches without qm (the species' ratios written on the device) give the same run
+    c = case_cls(p, max_batches=6)
+    c.load(*host[0])
+    rows_c = torch.empty((4, c.hist_cols), dtype=torch.float64).pin_memory()
+    HostPipeline(c, 2 * p.n_per_batch).run([h[:4] + h[5:] for h in host], rows_c)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(c.rho(), b.rho())
+    np.testing.assert_array_equal(rows_c.numpy(), rows.numpy())
+    with pytest.raises(ValueError):
+        HostPipeline(c, 2 * p.n_per_batch).run([h[:3] for h in host])
 
 
 def test_autotuners_pick_a_shape_and_keep_results(case_cls):

@@ -15,7 +15,9 @@
 //    Grids too large for shared memory read the same layout from global memory
 //    (L2-resident).
 //  * Persistent warps, one particle per lane, lanes refill from a global atomic
-//    queue as soon as their particle ends (no lane waits for a slow electron).
+//    queue as soon as their particle ends (no lane waits for a slow electron); a warp
+//    reserves a small block of ranks at a time and prefetches their particles into
+//    L1, so most refills wait neither for the atomic nor for the particle's loads.
 //  * Absorbed particles are deposited with integer atomics (bit-exact counts).
 //  * The x/y-symmetric arithmetic of a step (half-cell shift, the bilinear sums of
 //    (Ex, Ey), acceleration, velocity and position updates, cell remainder) runs on
@@ -482,27 +484,58 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     q.base = -1;
     q.c00 = q.c01 = q.c10 = q.c11 = tb_fcell{0.f, 0.f};
     bool open = true;
+    // The warp's reserved block of claim ranks [wc, we): empty lanes are refilled from it
+    // without an atomic, and a new block is reserved only when it runs short.  While the
+    // queue is long a block keeps up to one rank per lane beyond the lanes being served
+    // (guided: the reserve shrinks with the work left, so little is held back from other
+    // warps at the end), and the particle data of the kept ranks is prefetched into L1, so
+    // a refill waits neither for the queue atomic nor for the particle's loads.
+    unsigned long long wc = 0, we = 0;
+    const unsigned long long n_all = (unsigned long long)a.n;
+    const unsigned long long warps_all = (unsigned long long)gridDim.x * (blockDim.x >> 5);
 
     for (;;) {
-        // Refill empty lanes from the global queue (one atomic per warp) or leave once
-        // the queue is drained.
         unsigned need = __ballot_sync(FULL, s.pid < 0);
         if (need != 0u) {
-            if (!open) {
+            if (!open && wc >= we) {
                 if (pool != nullptr || need == FULL) break;
             } else {
-                const int leader = __ffs(need) - 1;
-                const int cnt = __popc(need);
-                unsigned long long base = 0;
-                if (lane == leader) base = atomicAdd(queue, (unsigned long long)cnt);
-                base = __shfl_sync(FULL, base, leader);
-                if (base + (unsigned long long)cnt >= (unsigned long long)a.n) open = false;
+                const unsigned cnt = __popc(need);
+                const unsigned long long avail = we - wc;
+                const bool reserve = avail < cnt && open;
+                unsigned long long nb = 0, nwc = wc + (avail < cnt ? avail : cnt), nwe = we;
+                if (reserve) {
+                    const unsigned long long left = n_all > we ? n_all - we : 0ULL;
+                    const unsigned long long extra = min(32ULL, left / (4ULL * warps_all));
+                    const unsigned long long size = (cnt - avail) + extra;
+                    const int leader = __ffs(need) - 1;
+                    if (lane == leader) nb = atomicAdd(queue, size);
+                    nb = __shfl_sync(FULL, nb, leader);
+                    if (nb + size >= n_all) open = false;
+                    nwc = nb + (cnt - avail);
+                    nwe = nb + size;
+                    // prefetch the particle data of the ranks kept for later refills
+                    const unsigned long long r = nwc + 8ULL * (unsigned)lane;
+                    if (r < nwe && r < n_all) {
+                        const unsigned long long i = k.reverse ? n_all - 1 - r : r;
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_x + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_y + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_vx + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_vy + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_qm + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_steps + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_status + i));
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_spc + i));
+                        if (RF) asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_clock + 2 * i));
+                    }
+                }
                 if (s.pid < 0) {
+                    // the j-th empty lane takes the block's next rank, then the reservation's
+                    const unsigned j = __popc(need & ((1u << lane) - 1u));
+                    const unsigned long long rank = j < avail ? wc + j : (reserve ? nb + (j - avail) : n_all);
                     // claim order: index order, or from the last index down (k.reverse)
-                    const unsigned long long rank = base + __popc(need & ((1u << lane) - 1u));
-                    const unsigned long long idx =
-                        (k.reverse && rank < (unsigned long long)a.n) ? (unsigned long long)a.n - 1 - rank : rank;
-                    if (idx < (unsigned long long)a.n && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
+                    const unsigned long long idx = (k.reverse && rank < n_all) ? n_all - 1 - rank : rank;
+                    if (idx < n_all && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
                         const int pid = (int)idx;
                         s.pid = pid;
                         q.base = -1;
@@ -528,6 +561,8 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                         }
                     }
                 }
+                wc = nwc;
+                we = nwe;
             }
             need = __ballot_sync(FULL, s.pid < 0);
         }

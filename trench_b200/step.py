@@ -24,7 +24,7 @@ from . import _capi, geometry, steady
 from .fields import (FieldSolver, apply_matrix, boundary_rhs, compute_field, conductor_surface_charge,
                      field_snapshot, field_voltages)
 from .inject import inject, launch_times
-from .params import E_CHARGE, EPS0, WALL_MODELS, is_tapered
+from .params import AMU, E_CHARGE, EPS0, M_E, WALL_MODELS, is_tapered
 from .tracer import DEFAULT_VSCALE, Context, _ptr
 
 CLAIM_ORDERS = ("index", "reverse")     # tb_set_claim_order 0, 1
@@ -872,7 +872,14 @@ class HostPipeline:
     """Batches from pinned host memory with the copy of batch k+1 overlapping the
     compute of batch k: two input buffer sets, one CUDA graph per set, a copy stream.
     The reference's loop (trench_charging_2d.py:1225-1285) copies and computes one
-    batch after the other."""
+    batch after the other.
+
+    A batch is (x, y, vx, vy, qm, spc) like the reference's, or (x, y, vx, vy, spc): then
+    each particle's charge-to-mass ratio is its species' (ions e / (ion_mass_amu u),
+    electrons -e / m_e, as the reference's inject draws them, trench_charging_2d.py:
+    458-489) and is written on the device from the species, so the host link carries
+    33 of the 41 bytes per particle (the link, about 22 GB/s from pinned memory on the
+    B200 hosts measured, is slower than the tracer at 41 bytes)."""
 
     def __init__(self, case, n):
         self.case = case
@@ -883,17 +890,28 @@ class HostPipeline:
         self.copied = [torch.cuda.Event(), torch.cuda.Event()]
         self.done = [torch.cuda.Event(), torch.cuda.Event()]
         self.row_dev = [torch.empty(case.hist_cols, dtype=torch.float64, device=case.dev) for _ in range(2)]
+        qm_ion = E_CHARGE / (case.p.ion_mass_amu * AMU)
+        self.qm_species = (torch.tensor(qm_ion, dtype=torch.float64, device=case.dev),
+                           torch.tensor(-E_CHARGE / M_E, dtype=torch.float64, device=case.dev))
 
     def _stage(self, k, batch, after):
         X, SPC = self.case._inputs[k % 2]
+        if len(batch) not in (5, 6):
+            raise ValueError("a batch is (x, y, vx, vy, qm, spc) or (x, y, vx, vy, spc)")
         self.copy.wait_event(after)
         with torch.cuda.stream(self.copy):
-            for dst, src in zip(X + [SPC], batch):
-                dst[:self.n].copy_(src, non_blocking=True)
+            if len(batch) == 6:
+                for dst, src in zip(X + [SPC], batch):
+                    dst[:self.n].copy_(src, non_blocking=True)
+            else:
+                for dst, src in zip(X[:4] + [SPC], batch):
+                    dst[:self.n].copy_(src, non_blocking=True)
+                torch.where(SPC[:self.n] == 0, self.qm_species[0], self.qm_species[1], out=X[4][:self.n])
             self.copied[k % 2].record(self.copy)
 
     def run(self, batches, rows=None, between=None):
-        """batches: list of (x, y, vx, vy, qm, spc) pinned host tensors of n particles each.
+        """batches: list of pinned host tensors of n particles each, (x, y, vx, vy, qm, spc)
+        or (x, y, vx, vy, spc) with the species' charge-to-mass ratios.
         rows: optional pinned (len(batches), hist_cols) tensor receiving each batch's
         history row.  between: optional callable run on the compute stream between batches."""
         comp = torch.cuda.current_stream(self.case.dev)
