@@ -908,9 +908,11 @@ def apply_tracer_setting(case, setting, n, reps=3):
     t, c = (int(v) for v in shape.split("x"))
     L = _capi.lib()
     case.ctx.check(L.tb_set_tuning(case.ctx.handle, t, c))
-    case.ctx.check(L.tb_set_claim_order(case.ctx.handle, 1 if order == "reverse" else 0))
+    from trench_b200.step import CLAIM_ORDERS
+    code = CLAIM_ORDERS.index(order) if order else 0
+    case.ctx.check(L.tb_set_claim_order(case.ctx.handle, code))
     case.tuning["tracer_shape"] = (t, c)
-    case.tuning["claim_order"] = "reverse" if order == "reverse" else "index"
+    case.tuning["claim_order"] = CLAIM_ORDERS[code]
 
 
 def device_injection(case, p, steps):
@@ -1138,7 +1140,7 @@ def main():
     ap.add_argument("--rf-batches", type=int, default=0,
                     help="rf_cycle workload: cap every leg at this many batches (0: the full 3000)")
     ap.add_argument("--tracer-shape", default="auto",
-                    help="auto (autotuned) or <threads>x<CTAs per SM>[-reverse], e.g. 1024x1-reverse")
+                    help="auto (autotuned) or <threads>x<CTAs per SM>[-reverse|-learned], e.g. 1024x1-reverse")
     ap.add_argument("--no-steady", dest="steady", action="store_false",
                     help="skip the run to steady charge (AR-8 workload, 1 GPU only)")
     ap.add_argument("--no-adjoint", dest="adjoint", action="store_false",

@@ -120,11 +120,16 @@ int tb_trace(tb_ctx *ctx, const tb_trace_args *args, int precision, void *stream
  * autotuner (ChargingCase.autotune_tracer). */
 int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
 /* Order in which the FP32 tracer's lanes claim particles: 0 in index order
- * (default), 1 from the last index down.  Results do not depend on it; the time
- * does, because the launch ends with the longest trajectories claimed last (in a
- * batch of ions then electrons whose electrons run longest, reverse order drains
- * sooner).  Chosen by the autotuner. */
-int tb_set_claim_order(tb_ctx *ctx, int reverse);
+ * (default), 1 from the last index down, 2 learned: every electron first, then the
+ * ions longest predicted first, the prediction being the mean step count of the ion's
+ * bin (starting column band, direction band) in the previous trace on this context
+ * (three small kernels before the trace write claim records in that order, two after
+ * it learn the bins; circuit_rf launches claim in index order).  Results do not depend
+ * on the order; the time does, because a launch ends with the particles still in
+ * flight when the queue runs dry.  The learned order's buffers are allocated by the
+ * first trace that uses it outside a stream capture (a capture before that claims in
+ * index order).  Chosen by the autotuner. */
+int tb_set_claim_order(tb_ctx *ctx, int order);
 
 /* Synchronise `stream`, then read and clear the context's device-side check flag:
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the

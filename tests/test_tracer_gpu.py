@@ -256,6 +256,32 @@ def test_chunked_run_with_stop_equals_single_launch(tracers):
         np.testing.assert_array_equal(u, v)
 
 
+def test_learned_claim_order_gives_the_same_outcomes(cuda_device):
+    """Claim order 2 (electrons first, then ions longest predicted first, learned from the
+    previous trace; particles claimed through FP32 claim records) changes only which lane
+    takes which particle: every particle's status, absorbing cell and step count equal the
+    index-order trace, on the first trace (nothing learned yet) and the next two."""
+    from trench_b200 import _capi
+    from trench_b200.tracer import B200Tracer
+    g = load_golden("trace_cfg2.npz")
+    p, solid = g["p"], g["solid"]
+    rng = np.random.default_rng(99)
+    batches = [inject.inject(p, 1 << 15, solid.shape[1], rng) for _ in range(3)]
+    plain = B200Tracer(~solid, cuda_device, precision="f32")
+    learned = B200Tracer(~solid, cuda_device, precision="f32")
+    args = (g["Ex"], g["Ey"], ~solid, p, barrier(g))
+    learned(*batches[0], *args)                       # creates the tracer's context
+    learned.ctx.check(_capi.lib().tb_set_claim_order(learned.ctx.handle, 2))
+    for b in batches:
+        want = plain(*b, *args)
+        w = plain.last
+        got = learned(*b, *args)
+        for a_, b_ in zip(want, got):
+            np.testing.assert_array_equal(a_, b_)
+        for k in ("status", "hit", "steps"):
+            np.testing.assert_array_equal(learned.last[k], w[k])
+
+
 def test_f64_quotients_by_a_known_reciprocal_equal_the_division(cuda_device):
     """The FP64 tracer divides by the cell size and the RF period through the rounded
     reciprocal and one exact correction; on 2^26 seeded pairs of each of three families

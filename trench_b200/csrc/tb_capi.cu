@@ -36,6 +36,11 @@ static int release(tb_ctx *c) {
     cudaFree(c->d_rf_wave);
     cudaFree(c->d_rf_barrier);
     cudaFree(c->d_queue);
+    cudaFree(c->d_claim_rec);
+    cudaFree(c->d_claim_key);
+    cudaFree(c->d_claim_cls);
+    cudaFree(c->d_ion_acc);
+    cudaFree(c->d_ion_class);
     cudaFree(c->d_err);
     tb_poisson_free(c->poisson);
     if (prev >= 0) cudaSetDevice(prev);

@@ -99,6 +99,13 @@ __device__ __forceinline__ void tb_store_packed(tb_fcell *out, const uint8_t *va
 struct tb_poisson;
 void tb_poisson_free(tb_poisson *ps);
 
+// Learned claim order of the FP32 tracer (tb_set_claim_order 2): ions are binned by
+// starting column band and direction, each bin's mean step count is learned from the
+// previous trace, and the particles are claimed electrons first, then ions longest
+// predicted first, through a table of claim records written in that order.
+constexpr int TB_ORDER_ION_BINS = 256;   // 64 column bands x 4 direction bands
+constexpr int TB_ORDER_CLASSES = 16;     // class 0 electrons, 1..15 ions by predicted length
+
 struct tb_ctx {
     int device = 0;
     int nx = 0, ny = 0;
@@ -117,7 +124,13 @@ struct tb_ctx {
     int smem_per_sm = 0;                 // shared memory of one SM (bytes)
     int tune_threads = 0;                // FP32 tracer CTA size (tb_set_tuning), 0 = by batch size
     int tune_ctas_per_sm = 1;            // FP32 tracer CTAs per SM
-    int tune_reverse = 0;                // FP32 tracer claims particles from the last index down
+    int tune_reverse = 0;                // FP32 tracer claim order: 0 index, 1 from the last index down, 2 learned
+    uint4 *d_claim_rec = nullptr;        // learned order: claim records (2 x uint4 per eligible particle)
+    uint16_t *d_claim_key = nullptr;     // learned order: each particle's ion bin (0xffff: electron / not traced)
+    long long claim_cap = 0;             // particles the two arrays above hold
+    unsigned *d_claim_cls = nullptr;     // learned order: class counts, starts, fill levels, eligible total
+    unsigned *d_ion_acc = nullptr;       // learned order: per ion bin step sum and count of the last trace
+    uint8_t *d_ion_class = nullptr;      // learned order: class of each ion bin for the next trace
     float4 *d_rf_field = nullptr;        // circuit_rf basis fields (exs, eys, exm, eym) x vac, halo-padded
     float4 *d_rf_barrier = nullptr;      // (2, nx*ny) per-face wall barrier of each basis potential
     int rf_ready = 0;

@@ -18,6 +18,9 @@
 //    queue as soon as their particle ends (no lane waits for a slow electron); a warp
 //    reserves a small block of ranks at a time and prefetches their particles into
 //    L1, so most refills wait neither for the atomic nor for the particle's loads.
+//  * Claim order (tb_set_claim_order): index, reverse, or learned -- electrons first,
+//    then ions longest predicted first from per-bin step means of the previous trace,
+//    claimed through FP32 claim records written in that order by a scatter kernel.
 //  * Absorbed particles are deposited with integer atomics (bit-exact counts).
 //  * The x/y-symmetric arithmetic of a step (half-cell shift, the bilinear sums of
 //    (Ex, Ey), acceleration, velocity and position updates, cell remainder) runs on
@@ -50,6 +53,8 @@ struct K32 {
     int bytes;                      // packed field bytes (multiple of 16)
     int pool_off;                   // byte offset of the drain pool in dynamic shared memory, -1 = none
     int reverse;                    // claim particles from the last index down
+    const uint4 *rec;               // learned order: claim records in claim order (nullptr = none)
+    const unsigned *n_rec;          // learned order: number of records (device)
     // circuit_rf in flight (kernels with RF = true): the unit-voltage basis fields
     // (exs, eys, exm, eym) x vac in field units per padded cell, their per-face wall
     // barriers (substrate basis then mask basis, nx*ny each), the waveform per table
@@ -453,7 +458,7 @@ __device__ __forceinline__ void pool_get(const uint32_t *P, int T, int q, LaneSt
 // rounds: the live particles are packed into the first warps, those warps take up
 // to TAIL_ROUND_STEPS steps, and the rest wait at the barrier.  A particle's
 // arithmetic does not depend on its lane, so the results are the same either way.
-template <bool SMEM, bool RF>
+template <bool SMEM, bool RF, bool REC = false>
 __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, uint32_t *pool) {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -491,7 +496,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     // warps at the end), and the particle data of the kept ranks is prefetched into L1, so
     // a refill waits neither for the queue atomic nor for the particle's loads.
     unsigned long long wc = 0, we = 0;
-    const unsigned long long n_all = (unsigned long long)a.n;
+    const unsigned long long n_all = REC ? (unsigned long long)*k.n_rec : (unsigned long long)a.n;
     const unsigned long long warps_all = (unsigned long long)gridDim.x * (blockDim.x >> 5);
 
     for (;;) {
@@ -515,8 +520,13 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                     nwc = nb + (cnt - avail);
                     nwe = nb + size;
                     // prefetch the particle data of the ranks kept for later refills
+                    if (REC) {
+                        // four 32-byte records to a 128-byte line
+                        const unsigned long long r = nwc + 4ULL * (unsigned)lane;
+                        if (r < nwe && r < n_all) asm volatile("prefetch.global.L1 [%0];" ::"l"(k.rec + 2 * r));
+                    }
                     const unsigned long long r = nwc + 8ULL * (unsigned)lane;
-                    if (r < nwe && r < n_all) {
+                    if (!REC && r < nwe && r < n_all) {
                         const unsigned long long i = k.reverse ? n_all - 1 - r : r;
                         asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_x + i));
                         asm volatile("prefetch.global.L1 [%0];" ::"l"(a.d_y + i));
@@ -533,9 +543,25 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
                     // the j-th empty lane takes the block's next rank, then the reservation's
                     const unsigned j = __popc(need & ((1u << lane) - 1u));
                     const unsigned long long rank = j < avail ? wc + j : (reserve ? nb + (j - avail) : n_all);
+                    if (REC && rank < n_all) {
+                        // learned order: the record holds the particle's FP32 start state,
+                        // converted by the scatter with the expressions below
+                        const uint4 r0 = __ldg(k.rec + 2 * rank), r1 = __ldg(k.rec + 2 * rank + 1);
+                        s.pid = (int)r0.x;
+                        q.base = -1;
+                        s.ix = (int)(r0.y & 0xffffu);
+                        s.iy = (int)r0.y >> 16;  // arithmetic shift keeps a negative row
+                        s.o = make_float2(__uint_as_float(r0.z), __uint_as_float(r0.w));
+                        s.v = make_float2(__uint_as_float(r1.x), __uint_as_float(r1.y));
+                        s.qm = __uint_as_float(r1.z);
+                        s.spc = (int)(r1.w >> 31);
+                        s.steps = (int)(r1.w & 0x7fffffffu);
+                        s.stop_at = min(a.max_steps, s.steps + a.step_budget);
+                        t.steps -= (unsigned)s.steps;
+                    }
                     // claim order: index order, or from the last index down (k.reverse)
                     const unsigned long long idx = (k.reverse && rank < n_all) ? n_all - 1 - rank : rank;
-                    if (idx < n_all && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
+                    if (!REC && idx < n_all && a.d_status[idx] == 3 && a.d_steps[idx] < a.max_steps) {
                         const int pid = (int)idx;
                         s.pid = pid;
                         q.base = -1;
@@ -623,7 +649,7 @@ __device__ __forceinline__ void run_case(const K32 &k, const tb_fcell *fieldp, u
     }
 }
 
-template <bool SMEM, int THREADS, bool RF>
+template <bool SMEM, int THREADS, bool RF, bool REC = false>
 __global__ void __launch_bounds__(THREADS, 1) trace_f32_kernel(const __grid_constant__ K32 k) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t mbar;
@@ -636,7 +662,7 @@ __global__ void __launch_bounds__(THREADS, 1) trace_f32_kernel(const __grid_cons
         fieldp = reinterpret_cast<const tb_fcell *>(smem_raw);
     }
     uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
-    run_case<SMEM, RF>(k, fieldp, pool);
+    run_case<SMEM, RF, REC>(k, fieldp, pool);
 }
 
 // Many cases in one persistent launch: each CTA repeatedly takes the case with the
@@ -793,7 +819,10 @@ int tb_configure_trace_f32(tb_ctx *ctx) {
     const int limit = ctx->max_smem - 1024;
 #define TB_SMEM_ATTR(T, RF)                                                                                  \
     TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, T, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                      limit))
+                                      limit));                                                               \
+    if (!RF)                                                                                                 \
+    TB_CUDA(ctx, cudaFuncSetAttribute(trace_f32_kernel<true, T, false, true>,                                \
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, limit))
     TB_SMEM_ATTR(1024, false);
     TB_SMEM_ATTR(768, false);
     TB_SMEM_ATTR(512, false);
@@ -829,7 +858,9 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.err = ctx->d_err;
     k.bytes = tb_halo_count(ctx->nx, ctx->ny) * (int)sizeof(tb_fcell);
     k.pool_off = -1;
-    k.reverse = ctx->tune_reverse;
+    k.reverse = ctx->tune_reverse == 1;
+    k.rec = nullptr;
+    k.n_rec = nullptr;
     k.rf_field = ctx->d_rf_field;
     k.rf_barrier = ctx->d_rf_barrier;
     k.rf_wave = ctx->d_rf_wave;
@@ -852,12 +883,206 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
 // Bytes of the drain pool for a block of `threads`.
 int pool_bytes(int threads, bool rf = false) { return (rf ? POOL_WORDS_RF : POOL_WORDS) * 4 * threads; }
 
+// ---- learned claim order ----------------------------------------------------------------
+// A launch ends with the particles still in flight when the queue runs dry.  Claimed in
+// index order the ions of a batch come last in random columns, and those above the
+// opening travel the whole trench (three to four times the steps of those stopped by the
+// mask), so they set the end.  The learned order claims every electron first (in index
+// order, as the reverse order does for a batch of ions then electrons) and then the ions
+// longest predicted first; the prediction is the mean step count of the ion's bin (64
+// starting column bands x 4 bands of vx / |vy|) in the previous trace on this context.
+constexpr uint16_t KEY_NONE = 0xffff, KEY_ELECTRON = 0xfffe;
+
+__device__ __forceinline__ int ion_bin(double x, double vx, double vy, double inv_lx) {
+    const int xb = min(max((int)(x * inv_lx * 64.0), 0), 63);
+    const double h = 0.1 * fabs(vy);
+    const int db = vx < 0.0 ? (vx < -h ? 0 : 1) : (vx > h ? 3 : 2);
+    return xb * 4 + db;
+}
+
+__device__ __forceinline__ int claim_class(uint16_t key, const uint8_t *ion_class) {
+    return key == KEY_NONE ? TB_ORDER_CLASSES : (key == KEY_ELECTRON ? 0 : 1 + ion_class[key]);
+}
+
+// Each particle's key (ion bin, electron, or not traced) and the particle count of each
+// class (cls[0..15]; warp-aggregated shared-memory counts, one global add per block).
+__global__ void k_claim_bins(const K32 k, double inv_lx, uint16_t *key, const uint8_t *ion_class, unsigned *cls) {
+    __shared__ unsigned h[TB_ORDER_CLASSES];
+    const tb_trace_args &a = k.a;
+    if (threadIdx.x < TB_ORDER_CLASSES) h[threadIdx.x] = 0;
+    __syncthreads();
+    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < a.n; i0 += (long long)gridDim.x * blockDim.x) {
+        const long long i = i0 + threadIdx.x;
+        int c = TB_ORDER_CLASSES;
+        if (i < a.n) {
+            uint16_t kk = KEY_NONE;
+            if (a.d_status[i] == 3 && a.d_steps[i] < a.max_steps)
+                kk = a.d_spc[i] ? KEY_ELECTRON : (uint16_t)ion_bin(a.d_x[i], a.d_vx[i], a.d_vy[i], inv_lx);
+            key[i] = kk;
+            c = claim_class(kk, ion_class);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        if (c < TB_ORDER_CLASSES && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[c], __popc(peers));
+    }
+    __syncthreads();
+    if (threadIdx.x < TB_ORDER_CLASSES && h[threadIdx.x]) atomicAdd(&cls[threadIdx.x], h[threadIdx.x]);
+}
+
+// Start of each class in the claim order (cls[16..31]), fill levels cleared (cls[32..47]),
+// the number of records (cls[48]); the counts are cleared for the next launch.
+__global__ void k_claim_scan(unsigned *cls) {
+    if (threadIdx.x == 0) {
+        unsigned off = 0;
+        for (int c = 0; c < TB_ORDER_CLASSES; ++c) {
+            cls[TB_ORDER_CLASSES + c] = off;
+            off += cls[c];
+            cls[c] = 0;
+            cls[2 * TB_ORDER_CLASSES + c] = 0;
+        }
+        cls[3 * TB_ORDER_CLASSES] = off;
+    }
+}
+
+// Each traced particle's claim record at its place in the claim order: the FP32 start
+// state converted with the claim's expressions (cell, offset, velocity in vscale units,
+// q/m), the step count and species, and the particle index.
+__global__ void k_claim_scatter(const K32 k, const uint16_t *key, const uint8_t *ion_class, unsigned *cls, uint4 *rec) {
+    const tb_trace_args &a = k.a;
+    const int lane = threadIdx.x & 31;
+    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < a.n; i0 += (long long)gridDim.x * blockDim.x) {
+        const long long i = i0 + threadIdx.x;
+        const int c = i < a.n ? claim_class(key[i], ion_class) : TB_ORDER_CLASSES;
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const int leader = __ffs(peers) - 1;
+        unsigned base = 0;
+        if (lane == leader && c < TB_ORDER_CLASSES) base = atomicAdd(&cls[2 * TB_ORDER_CLASSES + c], __popc(peers));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (c < TB_ORDER_CLASSES) {
+            const unsigned slot = cls[TB_ORDER_CLASSES + c] + base + __popc(peers & ((1u << lane) - 1u));
+            const double xc = a.d_x[i] * k.inv_dx, yc = a.d_y[i] * k.inv_dx;
+            const int ix = min(max((int)xc, 0), k.nx - 1);
+            const int iy = min((int)floor(yc), k.ny - 1);
+            const float ox = fminf(fmaxf((float)(xc - (double)ix), 0.f), ONE_BELOW);
+            const float oy = fminf(fmaxf((float)(yc - (double)iy), 0.f), ONE_BELOW);
+            const float vx = (float)(a.d_vx[i] * k.inv_v64), vy = (float)(a.d_vy[i] * k.inv_v64);
+            const float qm = (float)a.d_qm[i];
+            const unsigned st = (unsigned)a.d_steps[i] | (a.d_spc[i] ? 0x80000000u : 0u);
+            rec[2 * (size_t)slot] = make_uint4((unsigned)i, ((unsigned)ix & 0xffffu) | ((unsigned)iy << 16),
+                                               __float_as_uint(ox), __float_as_uint(oy));
+            rec[2 * (size_t)slot + 1] = make_uint4(__float_as_uint(vx), __float_as_uint(vy), __float_as_uint(qm), st);
+        }
+    }
+}
+
+// After the trace: step sum and count of each ion bin (shared-memory histogram per block,
+// one global add per bin and block).
+__global__ void __launch_bounds__(1024) k_claim_learn(long long n, const uint16_t *key, const int32_t *steps,
+                                                      unsigned *acc) {
+    __shared__ unsigned h[2 * TB_ORDER_ION_BINS];
+    for (int b = threadIdx.x; b < 2 * TB_ORDER_ION_BINS; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint16_t kk = key[i];
+        if (kk < TB_ORDER_ION_BINS) {
+            atomicAdd(&h[2 * kk], (unsigned)steps[i]);
+            atomicAdd(&h[2 * kk + 1], 1u);
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < 2 * TB_ORDER_ION_BINS; b += blockDim.x)
+        if (h[b]) atomicAdd(&acc[b], h[b]);
+}
+
+// Class of each ion bin for the next launch: 1 for the longest mean step count, then in
+// equal steps of that mean down to 15; bins without ions take the mean of all ions.  The
+// sums are cleared.
+__global__ void __launch_bounds__(TB_ORDER_ION_BINS) k_claim_classes(unsigned *acc, uint8_t *ion_class) {
+    __shared__ float s_sum[TB_ORDER_ION_BINS], s_cnt[TB_ORDER_ION_BINS], s_max[TB_ORDER_ION_BINS];
+    const int b = threadIdx.x;
+    const float sum = (float)acc[2 * b], cnt = (float)acc[2 * b + 1];
+    s_sum[b] = sum;
+    s_cnt[b] = cnt;
+    s_max[b] = cnt > 0.f ? sum / cnt : 0.f;
+    __syncthreads();
+    for (int o = TB_ORDER_ION_BINS / 2; o > 0; o >>= 1) {
+        if (b < o) {
+            s_sum[b] += s_sum[b + o];
+            s_cnt[b] += s_cnt[b + o];
+            s_max[b] = fmaxf(s_max[b], s_max[b + o]);
+        }
+        __syncthreads();
+    }
+    const float mean = s_cnt[0] > 0.f ? s_sum[0] / s_cnt[0] : 0.f, mx = s_max[0];
+    const float m = cnt > 0.f ? sum / cnt : mean;
+    const int c = mx > 0.f ? (int)(15.f * (1.f - m / (mx * 1.0001f))) : 0;
+    ion_class[b] = (uint8_t)min(max(c, 0), 14);
+    acc[2 * b] = 0u;
+    acc[2 * b + 1] = 0u;
+}
+
+// Learned-order buffers for n particles, allocated outside stream capture only; a failed
+// allocation leaves the order unused (the launch claims in index order).
+bool claim_buffers(tb_ctx *ctx, long long n, cudaStream_t s) {
+    if (ctx->d_claim_cls && n <= ctx->claim_cap) return true;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return false;
+    if (!ctx->d_claim_cls) {
+        unsigned *cls = nullptr, *acc = nullptr;
+        uint8_t *ion = nullptr;
+        const size_t cls_b = (3 * TB_ORDER_CLASSES + 1) * sizeof(unsigned), acc_b = 2 * TB_ORDER_ION_BINS * sizeof(unsigned);
+        const bool ok = cudaMalloc(&cls, cls_b) == cudaSuccess && cudaMalloc(&acc, acc_b) == cudaSuccess &&
+                        cudaMalloc(&ion, TB_ORDER_ION_BINS) == cudaSuccess && cudaMemset(cls, 0, cls_b) == cudaSuccess &&
+                        cudaMemset(acc, 0, acc_b) == cudaSuccess && cudaMemset(ion, 0, TB_ORDER_ION_BINS) == cudaSuccess;
+        if (!ok) {
+            cudaFree(cls);
+            cudaFree(acc);
+            cudaFree(ion);
+            cudaGetLastError();
+            return false;
+        }
+        ctx->d_claim_cls = cls;
+        ctx->d_ion_acc = acc;
+        ctx->d_ion_class = ion;
+    }
+    if (n > ctx->claim_cap) {
+        cudaFree(ctx->d_claim_rec);
+        cudaFree(ctx->d_claim_key);
+        ctx->d_claim_rec = nullptr;
+        ctx->d_claim_key = nullptr;
+        ctx->claim_cap = 0;
+        if (cudaMalloc(&ctx->d_claim_rec, (size_t)n * 2 * sizeof(uint4)) != cudaSuccess ||
+            cudaMalloc(&ctx->d_claim_key, (size_t)n * sizeof(uint16_t)) != cudaSuccess) {
+            cudaFree(ctx->d_claim_rec);
+            cudaFree(ctx->d_claim_key);
+            ctx->d_claim_rec = nullptr;
+            ctx->d_claim_key = nullptr;
+            cudaGetLastError();
+            return false;
+        }
+        ctx->claim_cap = n;
+    }
+    return true;
+}
+
 }  // namespace
 
 int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     K32 k = make_k32(ctx, a);
     const bool rf = a->n_phase > 0;
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
+    // learned claim order (not for circuit_rf launches): records written in claim order
+    const bool learned = ctx->tune_reverse == 2 && !rf && a->n > 0 && a->n <= 0x7fffffffLL && ctx->nx < 65536 &&
+                         ctx->ny < 32767 && claim_buffers(ctx, a->n, s);
+    const int oblocks = (int)std::min<long long>((a->n + 255) / 256, 4LL * std::max(ctx->num_sms, 1));
+    if (learned) {
+        const double inv_lx = 1.0 / (ctx->nx * ctx->dx);
+        k_claim_bins<<<oblocks, 256, 0, s>>>(k, inv_lx, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_cls);
+        k_claim_scan<<<1, 32, 0, s>>>(ctx->d_claim_cls);
+        k_claim_scatter<<<oblocks, 256, 0, s>>>(k, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_cls,
+                                                 ctx->d_claim_rec);
+        k.rec = ctx->d_claim_rec;
+        k.n_rec = ctx->d_claim_cls + 3 * TB_ORDER_CLASSES;
+    }
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
     int threads = ctx->tune_threads;
@@ -888,7 +1113,10 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
             if (smem) trace_f32_kernel<true, T, true><<<blocks, T, shm, s>>>(k);               \
             else trace_f32_kernel<false, T, true><<<blocks, T, shm, s>>>(k);                   \
         } else {                                                                                \
-            if (smem) trace_f32_kernel<true, T, false><<<blocks, T, shm, s>>>(k);              \
+            if (k.rec) {                                                                        \
+                if (smem) trace_f32_kernel<true, T, false, true><<<blocks, T, shm, s>>>(k);     \
+                else trace_f32_kernel<false, T, false, true><<<blocks, T, shm, s>>>(k);         \
+            } else if (smem) trace_f32_kernel<true, T, false><<<blocks, T, shm, s>>>(k);       \
             else trace_f32_kernel<false, T, false><<<blocks, T, shm, s>>>(k);                  \
         }                                                                                       \
     } while (0)
@@ -898,6 +1126,10 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     else if (threads == 768) TB_LAUNCH_F32(768);
     else TB_LAUNCH_F32(1024);
 #undef TB_LAUNCH_F32
+    if (learned) {
+        k_claim_learn<<<std::max(ctx->num_sms, 1), 1024, 0, s>>>(a->n, ctx->d_claim_key, a->d_steps, ctx->d_ion_acc);
+        k_claim_classes<<<1, TB_ORDER_ION_BINS, 0, s>>>(ctx->d_ion_acc, ctx->d_ion_class);
+    }
     TB_CUDA(ctx, cudaGetLastError());
     return TB_OK;
 }
@@ -1196,10 +1428,10 @@ extern "C" int tb_pack_check(tb_pack *p, void *stream) {
 }
 
 
-extern "C" int tb_set_claim_order(tb_ctx *ctx, int reverse) {
+extern "C" int tb_set_claim_order(tb_ctx *ctx, int order) {
     if (!ctx) return TB_ERR_ARG;
-    if (reverse != 0 && reverse != 1) return tb_fail(ctx, TB_ERR_ARG, "tb_set_claim_order: order must be 0 or 1");
-    ctx->tune_reverse = reverse;
+    if (order < 0 || order > 2) return tb_fail(ctx, TB_ERR_ARG, "tb_set_claim_order: order must be 0, 1 or 2");
+    ctx->tune_reverse = order;
     return TB_OK;
 }
 

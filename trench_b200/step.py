@@ -27,7 +27,7 @@ from .inject import inject, launch_times
 from .params import AMU, E_CHARGE, EPS0, M_E, WALL_MODELS, is_tapered
 from .tracer import DEFAULT_VSCALE, Context, _ptr
 
-CLAIM_ORDERS = ("index", "reverse")     # tb_set_claim_order 0, 1
+CLAIM_ORDERS = ("index", "reverse", "learned")     # tb_set_claim_order 0, 1, 2
 HIST_SCALARS = ("ratio_i_bottom", "ratio_e_bottom", "esc_e", "lost", "leak", "particle_steps")
 CHECKPOINT_VERSION = 1
 # settings a resumed run may change; everything else must equal the saved run's
@@ -510,7 +510,8 @@ class ChargingCase:
 
     def autotune_tracer(self, n=None, reps=2):
         """Times the tracer's launch shapes (CTA size, CTAs per SM) and claim orders (index
-        order or from the last index down) on the loaded batch and keeps the fastest.
+        order, from the last index down, or learned: electrons first, then ions longest
+        predicted first) on the loaded batch and keeps the fastest.
         Traces only: neither the charge state nor the loaded batch is changed (the trace
         is deterministic, so every setting gives the same counts)."""
         L = _capi.lib()
@@ -535,7 +536,7 @@ class ChargingCase:
         threads, per_sm, order = min(timings, key=timings.get)
         self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
         self.ctx.check(L.tb_set_claim_order(self.ctx.handle, order))
-        self.tuning["tracer"] = {f"{t}x{c}{'-reverse' if o else ''}": v for (t, c, o), v in timings.items()}
+        self.tuning["tracer"] = {f"{t}x{c}{'-' + CLAIM_ORDERS[o] if o else ''}": v for (t, c, o), v in timings.items()}
         self.tuning["tracer_shape"] = (threads, per_sm)
         self.tuning["claim_order"] = CLAIM_ORDERS[order]
         return timings
