@@ -910,7 +910,7 @@ def apply_tracer_setting(case, setting, n, reps=3):
     case.ctx.check(L.tb_set_tuning(case.ctx.handle, t, c))
     from trench_b200.step import CLAIM_ORDERS
     code = CLAIM_ORDERS.index(order) if order else 0
-    case.ctx.check(L.tb_set_claim_order(case.ctx.handle, code))
+    case.set_claim_order(code)
     case.tuning["tracer_shape"] = (t, c)
     case.tuning["claim_order"] = CLAIM_ORDERS[code]
 

@@ -126,10 +126,14 @@ int tb_set_tuning(tb_ctx *ctx, int threads, int ctas_per_sm);
  * (three small kernels before the trace write claim records in that order, two after
  * it learn the bins; circuit_rf launches claim in index order).  Results do not depend
  * on the order; the time does, because a launch ends with the particles still in
- * flight when the queue runs dry.  The learned order's buffers are allocated by the
- * first trace that uses it outside a stream capture (a capture before that claims in
- * index order).  Chosen by the autotuner. */
+ * flight when the queue runs dry.  The learned order's buffers are allocated by
+ * tb_reserve_claim_order or by the first trace that uses it outside a stream capture; a
+ * trace captured before either claims in index order.  Chosen by the autotuner. */
 int tb_set_claim_order(tb_ctx *ctx, int order);
+/* Allocates the learned claim order's buffers for batches of up to n particles (about
+ * 34 bytes per particle), so that a CUDA graph captured afterwards uses the order.  Not
+ * during a stream capture. */
+int tb_reserve_claim_order(tb_ctx *ctx, long long n);
 
 /* Synchronise `stream`, then read and clear the context's device-side check flag:
  * TB_ERR_KERNEL if a kernel recorded a failed bound (a deposit cell outside the

@@ -133,6 +133,7 @@ SIGNATURES = {
     "tb_check": (ctypes.c_int, [_vp, _vp]),
     "tb_set_tuning": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "tb_set_claim_order": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "tb_reserve_claim_order": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "tb_poisson_setup": (ctypes.c_int, [_vp, _vp, _vp, _vp, _vp, ctypes.c_int]),
     "tb_poisson_levels": (ctypes.c_int, [_vp]),
     "tb_poisson_schedule": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

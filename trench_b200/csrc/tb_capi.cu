@@ -39,6 +39,7 @@ static int release(tb_ctx *c) {
     cudaFree(c->d_claim_rec);
     cudaFree(c->d_claim_key);
     cudaFree(c->d_claim_cls);
+    cudaFree(c->d_claim_blk);
     cudaFree(c->d_ion_acc);
     cudaFree(c->d_ion_class);
     cudaFree(c->d_err);

@@ -128,7 +128,8 @@ struct tb_ctx {
     uint4 *d_claim_rec = nullptr;        // learned order: claim records (2 x uint4 per eligible particle)
     uint16_t *d_claim_key = nullptr;     // learned order: each particle's ion bin (0xffff: electron / not traced)
     long long claim_cap = 0;             // particles the two arrays above hold
-    unsigned *d_claim_cls = nullptr;     // learned order: class counts, starts, fill levels, eligible total
+    unsigned *d_claim_cls = nullptr;     // learned order: number of claim records
+    unsigned *d_claim_blk = nullptr;     // learned order: per block and class, particle count then start
     unsigned *d_ion_acc = nullptr;       // learned order: per ion bin step sum and count of the last trace
     uint8_t *d_ion_class = nullptr;      // learned order: class of each ion bin for the next trace
     float4 *d_rf_field = nullptr;        // circuit_rf basis fields (exs, eys, exm, eym) x vac, halo-padded

@@ -904,9 +904,18 @@ __device__ __forceinline__ int claim_class(uint16_t key, const uint8_t *ion_clas
     return key == KEY_NONE ? TB_ORDER_CLASSES : (key == KEY_ELECTRON ? 0 : 1 + ion_class[key]);
 }
 
-// Each particle's key (ion bin, electron, or not traced) and the particle count of each
-// class (cls[0..15]; warp-aggregated shared-memory counts, one global add per block).
-__global__ void k_claim_bins(const K32 k, double inv_lx, uint16_t *key, const uint8_t *ion_class, unsigned *cls) {
+// Blocks of the ordering kernels (k_claim_bins and k_claim_scatter walk the particles
+// with the same grid, so each block meets the same particles in both).
+constexpr int CLAIM_THREADS = 256;
+int claim_blocks(const tb_ctx *ctx, long long n) {
+    return (int)std::max<long long>(1, std::min<long long>((n + CLAIM_THREADS - 1) / CLAIM_THREADS,
+                                                           4LL * std::max(ctx->num_sms, 1)));
+}
+
+// Each particle's key (ion bin, electron, or not traced) and, per block, the number of
+// its particles in each class (blk[block][class]; warp-aggregated shared-memory counts).
+__global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k, double inv_lx, uint16_t *key,
+                                                              const uint8_t *ion_class, unsigned *blk) {
     __shared__ unsigned h[TB_ORDER_CLASSES];
     const tb_trace_args &a = k.a;
     if (threadIdx.x < TB_ORDER_CLASSES) h[threadIdx.x] = 0;
@@ -925,40 +934,81 @@ __global__ void k_claim_bins(const K32 k, double inv_lx, uint16_t *key, const ui
         if (c < TB_ORDER_CLASSES && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[c], __popc(peers));
     }
     __syncthreads();
-    if (threadIdx.x < TB_ORDER_CLASSES && h[threadIdx.x]) atomicAdd(&cls[threadIdx.x], h[threadIdx.x]);
+    if (threadIdx.x < TB_ORDER_CLASSES) blk[blockIdx.x * TB_ORDER_CLASSES + threadIdx.x] = h[threadIdx.x];
 }
 
-// Start of each class in the claim order (cls[16..31]), fill levels cleared (cls[32..47]),
-// the number of records (cls[48]); the counts are cleared for the next launch.
-__global__ void k_claim_scan(unsigned *cls) {
-    if (threadIdx.x == 0) {
+// One block of 1024 threads (thread b for ordering block b, nb <= 1024): the start of
+// each ordering block's share of each class in the claim order (classes in turn, blocks
+// in turn within a class), written over the counts, and the number of records.
+__global__ void __launch_bounds__(1024) k_claim_scan(unsigned *blk, int nb, unsigned *n_rec) {
+    __shared__ unsigned s_warp[32];
+    __shared__ unsigned s_tot[TB_ORDER_CLASSES], s_start[TB_ORDER_CLASSES];
+    const unsigned FULL = 0xffffffffu;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    unsigned excl[TB_ORDER_CLASSES];
+#pragma unroll
+    for (int c = 0; c < TB_ORDER_CLASSES; ++c) {
+        const unsigned v = t < nb ? blk[t * TB_ORDER_CLASSES + c] : 0u;
+        unsigned x = v;  // inclusive scan within the warp
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(FULL, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) s_warp[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            unsigned z = s_warp[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(FULL, z, o);
+                if (lane >= o) z += y;
+            }
+            s_warp[lane] = z;
+        }
+        __syncthreads();
+        const unsigned before = w > 0 ? s_warp[w - 1] : 0u;
+        excl[c] = before + x - v;
+        if (t == 0) s_tot[c] = s_warp[31];
+        __syncthreads();
+    }
+    if (t == 0) {
         unsigned off = 0;
         for (int c = 0; c < TB_ORDER_CLASSES; ++c) {
-            cls[TB_ORDER_CLASSES + c] = off;
-            off += cls[c];
-            cls[c] = 0;
-            cls[2 * TB_ORDER_CLASSES + c] = 0;
+            s_start[c] = off;
+            off += s_tot[c];
         }
-        cls[3 * TB_ORDER_CLASSES] = off;
+        *n_rec = off;
+    }
+    __syncthreads();
+    if (t < nb) {
+#pragma unroll
+        for (int c = 0; c < TB_ORDER_CLASSES; ++c) blk[t * TB_ORDER_CLASSES + c] = s_start[c] + excl[c];
     }
 }
 
 // Each traced particle's claim record at its place in the claim order: the FP32 start
 // state converted with the claim's expressions (cell, offset, velocity in vscale units,
-// q/m), the step count and species, and the particle index.
-__global__ void k_claim_scatter(const K32 k, const uint16_t *key, const uint8_t *ion_class, unsigned *cls, uint4 *rec) {
+// q/m), the step count and species, and the particle index.  Places are handed out from
+// the block's starts with shared-memory counters.
+__global__ void __launch_bounds__(CLAIM_THREADS) k_claim_scatter(const K32 k, const uint16_t *key,
+                                                                 const uint8_t *ion_class, const unsigned *blk,
+                                                                 uint4 *rec) {
+    __shared__ unsigned fill[TB_ORDER_CLASSES];
     const tb_trace_args &a = k.a;
     const int lane = threadIdx.x & 31;
+    if (threadIdx.x < TB_ORDER_CLASSES) fill[threadIdx.x] = blk[blockIdx.x * TB_ORDER_CLASSES + threadIdx.x];
+    __syncthreads();
     for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < a.n; i0 += (long long)gridDim.x * blockDim.x) {
         const long long i = i0 + threadIdx.x;
         const int c = i < a.n ? claim_class(key[i], ion_class) : TB_ORDER_CLASSES;
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         const int leader = __ffs(peers) - 1;
         unsigned base = 0;
-        if (lane == leader && c < TB_ORDER_CLASSES) base = atomicAdd(&cls[2 * TB_ORDER_CLASSES + c], __popc(peers));
+        if (lane == leader && c < TB_ORDER_CLASSES) base = atomicAdd(&fill[c], __popc(peers));
         base = __shfl_sync(0xffffffffu, base, leader);
         if (c < TB_ORDER_CLASSES) {
-            const unsigned slot = cls[TB_ORDER_CLASSES + c] + base + __popc(peers & ((1u << lane) - 1u));
+            const unsigned slot = base + __popc(peers & ((1u << lane) - 1u));
             const double xc = a.d_x[i] * k.inv_dx, yc = a.d_y[i] * k.inv_dx;
             const int ix = min(max((int)xc, 0), k.nx - 1);
             const int iy = min((int)floor(yc), k.ny - 1);
@@ -1027,20 +1077,24 @@ bool claim_buffers(tb_ctx *ctx, long long n, cudaStream_t s) {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return false;
     if (!ctx->d_claim_cls) {
-        unsigned *cls = nullptr, *acc = nullptr;
+        unsigned *cls = nullptr, *blk = nullptr, *acc = nullptr;
         uint8_t *ion = nullptr;
-        const size_t cls_b = (3 * TB_ORDER_CLASSES + 1) * sizeof(unsigned), acc_b = 2 * TB_ORDER_ION_BINS * sizeof(unsigned);
-        const bool ok = cudaMalloc(&cls, cls_b) == cudaSuccess && cudaMalloc(&acc, acc_b) == cudaSuccess &&
-                        cudaMalloc(&ion, TB_ORDER_ION_BINS) == cudaSuccess && cudaMemset(cls, 0, cls_b) == cudaSuccess &&
+        const size_t blk_b = (size_t)TB_ORDER_CLASSES * 4 * std::max(ctx->num_sms, 1) * sizeof(unsigned);
+        const size_t acc_b = 2 * TB_ORDER_ION_BINS * sizeof(unsigned);
+        const bool ok = cudaMalloc(&cls, sizeof(unsigned)) == cudaSuccess && cudaMalloc(&blk, blk_b) == cudaSuccess &&
+                        cudaMalloc(&acc, acc_b) == cudaSuccess && cudaMalloc(&ion, TB_ORDER_ION_BINS) == cudaSuccess &&
+                        cudaMemset(cls, 0, sizeof(unsigned)) == cudaSuccess && cudaMemset(blk, 0, blk_b) == cudaSuccess &&
                         cudaMemset(acc, 0, acc_b) == cudaSuccess && cudaMemset(ion, 0, TB_ORDER_ION_BINS) == cudaSuccess;
         if (!ok) {
             cudaFree(cls);
+            cudaFree(blk);
             cudaFree(acc);
             cudaFree(ion);
             cudaGetLastError();
             return false;
         }
         ctx->d_claim_cls = cls;
+        ctx->d_claim_blk = blk;
         ctx->d_ion_acc = acc;
         ctx->d_ion_class = ion;
     }
@@ -1072,16 +1126,16 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     TB_CUDA(ctx, cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), s));
     // learned claim order (not for circuit_rf launches): records written in claim order
     const bool learned = ctx->tune_reverse == 2 && !rf && a->n > 0 && a->n <= 0x7fffffffLL && ctx->nx < 65536 &&
-                         ctx->ny < 32767 && claim_buffers(ctx, a->n, s);
-    const int oblocks = (int)std::min<long long>((a->n + 255) / 256, 4LL * std::max(ctx->num_sms, 1));
+                         ctx->ny < 32767 && 4 * ctx->num_sms <= 1024 && claim_buffers(ctx, a->n, s);
     if (learned) {
         const double inv_lx = 1.0 / (ctx->nx * ctx->dx);
-        k_claim_bins<<<oblocks, 256, 0, s>>>(k, inv_lx, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_cls);
-        k_claim_scan<<<1, 32, 0, s>>>(ctx->d_claim_cls);
-        k_claim_scatter<<<oblocks, 256, 0, s>>>(k, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_cls,
-                                                 ctx->d_claim_rec);
+        const int nb = claim_blocks(ctx, a->n);  // at most 4 x SMs <= 1024, one scan thread each
+        k_claim_bins<<<nb, CLAIM_THREADS, 0, s>>>(k, inv_lx, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_blk);
+        k_claim_scan<<<1, 1024, 0, s>>>(ctx->d_claim_blk, nb, ctx->d_claim_cls);
+        k_claim_scatter<<<nb, CLAIM_THREADS, 0, s>>>(k, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_blk,
+                                                      ctx->d_claim_rec);
         k.rec = ctx->d_claim_rec;
-        k.n_rec = ctx->d_claim_cls + 3 * TB_ORDER_CLASSES;
+        k.n_rec = ctx->d_claim_cls;
     }
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
@@ -1427,6 +1481,14 @@ extern "C" int tb_pack_check(tb_pack *p, void *stream) {
     return TB_OK;
 }
 
+
+extern "C" int tb_reserve_claim_order(tb_ctx *ctx, long long n) {
+    if (!ctx || n < 0 || n > 0x7fffffffLL) return TB_ERR_ARG;
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (!claim_buffers(ctx, n > 0 ? n : 1, 0))
+        return tb_fail(ctx, TB_ERR_CUDA, "tb_reserve_claim_order: could not allocate the claim-order buffers for %lld particles", n);
+    return TB_OK;
+}
 
 extern "C" int tb_set_claim_order(tb_ctx *ctx, int order) {
     if (!ctx) return TB_ERR_ARG;

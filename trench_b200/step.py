@@ -508,6 +508,15 @@ class ChargingCase:
 
     TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2), (256, 1), (128, 1))
 
+    def set_claim_order(self, order):
+        """Sets the tracer's claim order (an index into CLAIM_ORDERS); the learned order's
+        buffers are reserved for the case's capacity, so graphs captured later use it."""
+        L = _capi.lib()
+        self.ctx.check(L.tb_set_claim_order(self.ctx.handle, int(order)))
+        if CLAIM_ORDERS[order] == "learned":
+            self.ctx.check(L.tb_reserve_claim_order(self.ctx.handle, self.capacity))
+        self.tuning["claim_order"] = CLAIM_ORDERS[order]
+
     def autotune_tracer(self, n=None, reps=2):
         """Times the tracer's launch shapes (CTA size, CTAs per SM) and claim orders (index
         order, from the last index down, or learned: electrons first, then ions longest
@@ -522,7 +531,7 @@ class ChargingCase:
         self.trace_events = (e0, e1)
         try:
             for order in range(len(CLAIM_ORDERS)):
-                self.ctx.check(L.tb_set_claim_order(self.ctx.handle, order))
+                self.set_claim_order(order)
                 for threads, per_sm in self.TRACER_SHAPES:
                     self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
                     best = float("inf")
@@ -535,7 +544,7 @@ class ChargingCase:
             self.trace_events = saved
         threads, per_sm, order = min(timings, key=timings.get)
         self.ctx.check(L.tb_set_tuning(self.ctx.handle, threads, per_sm))
-        self.ctx.check(L.tb_set_claim_order(self.ctx.handle, order))
+        self.set_claim_order(order)
         self.tuning["tracer"] = {f"{t}x{c}{'-' + CLAIM_ORDERS[o] if o else ''}": v for (t, c, o), v in timings.items()}
         self.tuning["tracer_shape"] = (threads, per_sm)
         self.tuning["claim_order"] = CLAIM_ORDERS[order]
