@@ -260,7 +260,8 @@ def test_learned_claim_order_gives_the_same_outcomes(cuda_device):
     """Claim order 2 (electrons first, then ions longest predicted first, learned from the
     previous trace; particles claimed through FP32 claim records) changes only which lane
     takes which particle: every particle's status, absorbing cell and step count equal the
-    index-order trace, on the first trace (nothing learned yet) and the next two."""
+    index-order trace on three batches, the first with the classes learned on the same
+    particles, the others on new ones."""
     from trench_b200 import _capi
     from trench_b200.tracer import B200Tracer
     g = load_golden("trace_cfg2.npz")
@@ -270,7 +271,9 @@ def test_learned_claim_order_gives_the_same_outcomes(cuda_device):
     plain = B200Tracer(~solid, cuda_device, precision="f32")
     learned = B200Tracer(~solid, cuda_device, precision="f32")
     args = (g["Ex"], g["Ey"], ~solid, p, barrier(g))
-    learned(*batches[0], *args)                       # creates the tracer's context
+    plain(*batches[0], *args)                         # creates the tracers' contexts
+    learned(*batches[0], *args)
+    plain.ctx.check(_capi.lib().tb_set_claim_order(plain.ctx.handle, 0))
     learned.ctx.check(_capi.lib().tb_set_claim_order(learned.ctx.handle, 2))
     for b in batches:
         want = plain(*b, *args)

@@ -939,42 +939,58 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k, doubl
 
 // One block of 1024 threads (thread b for ordering block b, nb <= 1024): the start of
 // each ordering block's share of each class in the claim order (classes in turn, blocks
-// in turn within a class), written over the counts, and the number of records.
+// in turn within a class), written over the counts, and the number of records.  Each
+// thread scans its 16 counts within its warp; warp c then scans the warps' totals of
+// class c.
 __global__ void __launch_bounds__(1024) k_claim_scan(unsigned *blk, int nb, unsigned *n_rec) {
-    __shared__ unsigned s_warp[32];
-    __shared__ unsigned s_tot[TB_ORDER_CLASSES], s_start[TB_ORDER_CLASSES];
+    constexpr int C = TB_ORDER_CLASSES;
+    __shared__ unsigned s_wsum[32][C + 1];   // per warp and class: the warp's total, then the warps before it
+    __shared__ unsigned s_tot[C], s_start[C];
     const unsigned FULL = 0xffffffffu;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    unsigned excl[TB_ORDER_CLASSES];
+    unsigned v[C], x[C];
+    if (t < nb) {
+        const uint4 *row = reinterpret_cast<const uint4 *>(blk + (size_t)t * C);
 #pragma unroll
-    for (int c = 0; c < TB_ORDER_CLASSES; ++c) {
-        const unsigned v = t < nb ? blk[t * TB_ORDER_CLASSES + c] : 0u;
-        unsigned x = v;  // inclusive scan within the warp
+        for (int q = 0; q < C / 4; ++q) {
+            const uint4 u = row[q];
+            v[4 * q] = u.x;
+            v[4 * q + 1] = u.y;
+            v[4 * q + 2] = u.z;
+            v[4 * q + 3] = u.w;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < C; ++c) v[c] = 0u;
+    }
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        unsigned y = v[c];  // inclusive scan within the warp
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const unsigned y = __shfl_up_sync(FULL, x, o);
-            if (lane >= o) x += y;
+            const unsigned z = __shfl_up_sync(FULL, y, o);
+            if (lane >= o) y += z;
         }
-        if (lane == 31) s_warp[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            unsigned z = s_warp[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned y = __shfl_up_sync(FULL, z, o);
-                if (lane >= o) z += y;
-            }
-            s_warp[lane] = z;
-        }
-        __syncthreads();
-        const unsigned before = w > 0 ? s_warp[w - 1] : 0u;
-        excl[c] = before + x - v;
-        if (t == 0) s_tot[c] = s_warp[31];
-        __syncthreads();
+        x[c] = y;
+        if (lane == 31) s_wsum[w][c] = y;
     }
+    __syncthreads();
+    if (w < C) {  // warp c: exclusive scan of class c over the 32 warps
+        const unsigned own = s_wsum[lane][w];
+        unsigned y = own;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned z = __shfl_up_sync(FULL, y, o);
+            if (lane >= o) y += z;
+        }
+        __syncwarp();
+        s_wsum[lane][w] = y - own;
+        if (lane == 31) s_tot[w] = y;
+    }
+    __syncthreads();
     if (t == 0) {
         unsigned off = 0;
-        for (int c = 0; c < TB_ORDER_CLASSES; ++c) {
+        for (int c = 0; c < C; ++c) {
             s_start[c] = off;
             off += s_tot[c];
         }
@@ -982,8 +998,16 @@ __global__ void __launch_bounds__(1024) k_claim_scan(unsigned *blk, int nb, unsi
     }
     __syncthreads();
     if (t < nb) {
+        uint4 *row = reinterpret_cast<uint4 *>(blk + (size_t)t * C);
 #pragma unroll
-        for (int c = 0; c < TB_ORDER_CLASSES; ++c) blk[t * TB_ORDER_CLASSES + c] = s_start[c] + excl[c];
+        for (int q = 0; q < C / 4; ++q) {
+            uint4 u;
+            u.x = s_start[4 * q] + s_wsum[w][4 * q] + x[4 * q] - v[4 * q];
+            u.y = s_start[4 * q + 1] + s_wsum[w][4 * q + 1] + x[4 * q + 1] - v[4 * q + 1];
+            u.z = s_start[4 * q + 2] + s_wsum[w][4 * q + 2] + x[4 * q + 2] - v[4 * q + 2];
+            u.w = s_start[4 * q + 3] + s_wsum[w][4 * q + 3] + x[4 * q + 3] - v[4 * q + 3];
+            row[q] = u;
+        }
     }
 }
 

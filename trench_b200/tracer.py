@@ -163,6 +163,10 @@ class B200Tracer:
         if self._ctx_dx != dx:
             self.ctx.close()
             self.ctx = Context(self.vac, self.device, dx)
+            # FP32 launches claim in the learned order (electrons first, then ions longest
+            # predicted first from the previous call): a call's time is set by the
+            # particles still in flight when its queue runs dry
+            self.ctx.check(_capi.lib().tb_set_claim_order(self.ctx.handle, 2))
             self._ctx_dx = dx
             self._packed = None
         return self.ctx
