@@ -924,9 +924,12 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k, doubl
         const long long i = i0 + threadIdx.x;
         int c = TB_ORDER_CLASSES;
         if (i < a.n) {
+            // every load of the particle issued at once (one memory round trip)
+            const int8_t st = a.d_status[i], sp = a.d_spc[i];
+            const int32_t n_steps = a.d_steps[i];
+            const double x = a.d_x[i], vx = a.d_vx[i], vy = a.d_vy[i];
             uint16_t kk = KEY_NONE;
-            if (a.d_status[i] == 3 && a.d_steps[i] < a.max_steps)
-                kk = a.d_spc[i] ? KEY_ELECTRON : (uint16_t)ion_bin(a.d_x[i], a.d_vx[i], a.d_vy[i], inv_lx);
+            if (st == 3 && n_steps < a.max_steps) kk = sp ? KEY_ELECTRON : (uint16_t)ion_bin(x, vx, vy, inv_lx);
             key[i] = kk;
             c = claim_class(kk, ion_class);
         }
@@ -1025,7 +1028,27 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_scatter(const K32 k, co
     __syncthreads();
     for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < a.n; i0 += (long long)gridDim.x * blockDim.x) {
         const long long i = i0 + threadIdx.x;
-        const int c = i < a.n ? claim_class(key[i], ion_class) : TB_ORDER_CLASSES;
+        int c = TB_ORDER_CLASSES;
+        uint4 r0 = make_uint4(0u, 0u, 0u, 0u), r1 = r0;
+        if (i < a.n) {
+            // the key and the particle's data loaded together (one memory round trip)
+            const uint16_t kk = key[i];
+            const double x = a.d_x[i], y = a.d_y[i], vx64 = a.d_vx[i], vy64 = a.d_vy[i], qm64 = a.d_qm[i];
+            const int32_t n_steps = a.d_steps[i];
+            const int8_t sp = a.d_spc[i];
+            c = claim_class(kk, ion_class);
+            const double xc = x * k.inv_dx, yc = y * k.inv_dx;
+            const int ix = min(max((int)xc, 0), k.nx - 1);
+            const int iy = min((int)floor(yc), k.ny - 1);
+            const float ox = fminf(fmaxf((float)(xc - (double)ix), 0.f), ONE_BELOW);
+            const float oy = fminf(fmaxf((float)(yc - (double)iy), 0.f), ONE_BELOW);
+            const float vx = (float)(vx64 * k.inv_v64), vy = (float)(vy64 * k.inv_v64);
+            const float qm = (float)qm64;
+            r0 = make_uint4((unsigned)i, ((unsigned)ix & 0xffffu) | ((unsigned)iy << 16), __float_as_uint(ox),
+                            __float_as_uint(oy));
+            r1 = make_uint4(__float_as_uint(vx), __float_as_uint(vy), __float_as_uint(qm),
+                            (unsigned)n_steps | (sp ? 0x80000000u : 0u));
+        }
         const unsigned peers = __match_any_sync(0xffffffffu, c);
         const int leader = __ffs(peers) - 1;
         unsigned base = 0;
@@ -1033,17 +1056,8 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_scatter(const K32 k, co
         base = __shfl_sync(0xffffffffu, base, leader);
         if (c < TB_ORDER_CLASSES) {
             const unsigned slot = base + __popc(peers & ((1u << lane) - 1u));
-            const double xc = a.d_x[i] * k.inv_dx, yc = a.d_y[i] * k.inv_dx;
-            const int ix = min(max((int)xc, 0), k.nx - 1);
-            const int iy = min((int)floor(yc), k.ny - 1);
-            const float ox = fminf(fmaxf((float)(xc - (double)ix), 0.f), ONE_BELOW);
-            const float oy = fminf(fmaxf((float)(yc - (double)iy), 0.f), ONE_BELOW);
-            const float vx = (float)(a.d_vx[i] * k.inv_v64), vy = (float)(a.d_vy[i] * k.inv_v64);
-            const float qm = (float)a.d_qm[i];
-            const unsigned st = (unsigned)a.d_steps[i] | (a.d_spc[i] ? 0x80000000u : 0u);
-            rec[2 * (size_t)slot] = make_uint4((unsigned)i, ((unsigned)ix & 0xffffu) | ((unsigned)iy << 16),
-                                               __float_as_uint(ox), __float_as_uint(oy));
-            rec[2 * (size_t)slot + 1] = make_uint4(__float_as_uint(vx), __float_as_uint(vy), __float_as_uint(qm), st);
+            rec[2 * (size_t)slot] = r0;
+            rec[2 * (size_t)slot + 1] = r1;
         }
     }
 }
