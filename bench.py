@@ -409,8 +409,10 @@ def run_b200(args, p):
             "large": large,
             "adjoint": adj,
             "to_steady": to_steady,
-            # per step: tracer, fused charge update, Green's GEMV, field, monitors
-            "gpu_launches": 5 * args.steps,
+            # per step: batch reset, tracer, fused charge update, Green's GEMV, field, monitors,
+            # and with the learned claim order its three ordering kernels before the tracer and
+            # two after it
+            "gpu_launches": step_launches(case) * args.steps,
             "roofline": roof, "cpu_baseline": cpu, "clocks": clk,
             "wall_s": wall}
     print(json.dumps(line), flush=True)
@@ -682,9 +684,9 @@ def large_measure(steps, warmup, n_per_species=1 << 23, tracer_shape="auto", cpu
                                 "its four corners while it stays in one cell quad, and two of them share a "
                                 "sector, so fewer sectors are fetched than the bytes counted"},
            "l2": "flushed between timed steps (256 MiB write)", "clocks": clk,
-           # per step: injection, tracer, deposit, leakage GEMV, finish (m > 1024: unfused charge
-           # update), Green's GEMV, field, monitors
-           "gpu_launches": 8 * steps,
+           # per step: injection, batch reset, tracer, deposit, leakage GEMV, finish (m > 1024:
+           # unfused charge update), Green's GEMV, field, monitors (+ 5 with the learned order)
+           "gpu_launches": (9 + (5 if case.tuning.get("claim_order") == "learned" else 0)) * steps,
            "cpu_baseline": large_cpu_baseline(case, p, seconds_budget=cpu_seconds)}
     if accuracy:
         inj()
@@ -809,8 +811,9 @@ def run_rf_cycle(args):
                     "h2d_bytes_per_step": n * (5 * 8 + 1 + 16), "d2h_bytes_per_step": d2h // max(hb, 1),
                     "note": "ChargingCase construction + run(rng) with host injection (NumPy PCG64) each batch"},
             "clocks": clk,
-            # per batch: injection, tracer, deposit, leakage GEMV, finish, Green's GEMV, field, monitors
-            "gpu_launches": 8 * nb}
+            # per batch: injection, batch reset, tracer, deposit, leakage GEMV, finish, Green's GEMV,
+            # field, monitors
+            "gpu_launches": 9 * nb}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -895,6 +898,13 @@ def run_standard(args):
             "clocks": clk, "gpu_launches": None}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def step_launches(case):
+    """This library's kernels in one device batch step of a ChargingCase with the fused
+    charge update: batch reset, tracer, charge, Green's GEMV, field, monitors, plus the
+    learned claim order's five ordering kernels."""
+    return 6 + (5 if case.tuning.get("claim_order") == "learned" else 0)
 
 
 def apply_tracer_setting(case, setting, n, reps=3):

@@ -219,6 +219,11 @@ int tb_step_potential(tb_ctx *ctx, const tb_step_desc *desc, void *stream);
  * Call after tb_step_charge. */
 int tb_step_monitors(tb_ctx *ctx, const tb_step_desc *desc, const double *d_weights, const uint8_t *d_absolute,
                      int n_monitors, double *d_out, void *stream);
+/* The per-batch state before a trace in one launch (the reference sets it per call,
+ * trench_cuda.py:73-74): d_status[0..n) = 3 (untraced), d_steps[0..n) = 0,
+ * d_counts[0..n_counts) = 0 and d_totals[0..n_totals) = 0 (n_totals <= 64). */
+int tb_batch_reset(tb_ctx *ctx, int8_t *d_status, int32_t *d_steps, long long n, int32_t *d_counts,
+                   long long n_counts, unsigned long long *d_totals, int n_totals, void *stream);
 
 /* ---- Device-side injection -------------------------------------------------------
  * Samples n_species ions (indices [0, n)) then n_species electrons ([n, 2n)) into the

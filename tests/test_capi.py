@@ -82,6 +82,7 @@ def test_entry_points_reject_a_missing_context(lib):
     assert lib.tb_set_tuning(null, 1024, 1) == _capi.TB_ERR_ARG
     assert lib.tb_set_claim_order(null, 0) == _capi.TB_ERR_ARG
     assert lib.tb_reserve_claim_order(null, 10) == _capi.TB_ERR_ARG
+    assert lib.tb_batch_reset(null, null, null, 0, null, 0, null, 0, null) == _capi.TB_ERR_ARG
     assert lib.tb_trace(null, null, 1, null) == _capi.TB_ERR_ARG
     assert lib.tb_check(null, null) == _capi.TB_ERR_ARG
     assert lib.tb_inject(null, null, null) == _capi.TB_ERR_ARG

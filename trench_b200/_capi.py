@@ -142,6 +142,7 @@ SIGNATURES = {
     "tb_step_charge": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_potential": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp]),
     "tb_step_monitors": (ctypes.c_int, [_vp, ctypes.POINTER(StepDesc), _vp, _vp, ctypes.c_int, _vp, _vp]),
+    "tb_batch_reset": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_longlong, _vp, ctypes.c_longlong, _vp, ctypes.c_int, _vp]),
     "tb_bench_smem": (ctypes.c_int, [_vp, ctypes.POINTER(_dbl)]),
     "tb_bench_l2_gather": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.POINTER(_dbl)]),
     "tb_check_div_by": (ctypes.c_int, [_vp, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_ulonglong)]),

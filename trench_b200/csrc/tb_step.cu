@@ -442,6 +442,39 @@ extern "C" int tb_step_potential(tb_ctx *ctx, const tb_step_desc *d, void *strea
     return TB_OK;
 }
 
+// The per-batch state before a trace, in one launch: every particle untraced (status 3,
+// no steps), the hit counts and the totals zero.
+__global__ void k_batch_reset(int8_t *status, int32_t *steps, long long n, int32_t *counts, long long n_counts,
+                              unsigned long long *totals, int n_totals) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long end = n > n_counts ? n : n_counts;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+        if (i < n) {
+            status[i] = 3;
+            steps[i] = 0;
+        }
+        if (i < n_counts) counts[i] = 0;
+        if (i < n_totals) totals[i] = 0ULL;
+    }
+}
+
+extern "C" int tb_batch_reset(tb_ctx *ctx, int8_t *d_status, int32_t *d_steps, long long n, int32_t *d_counts,
+                              long long n_counts, unsigned long long *d_totals, int n_totals, void *stream) {
+    if (!ctx || n < 0 || n_counts < 0 || n_totals < 0 || n_totals > 64 || (n > 0 && (!d_status || !d_steps)) ||
+        (n_counts > 0 && !d_counts) || (n_totals > 0 && !d_totals))
+        return tb_fail(ctx, TB_ERR_ARG, "tb_batch_reset: invalid arguments");
+    const long long end = std::max(std::max(n, n_counts), (long long)n_totals);
+    if (end == 0) return TB_OK;
+    TB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int threads = 256;
+    const long long want = (end + threads - 1) / threads;
+    const int blocks = (int)std::min<long long>(want, 8LL * std::max(ctx->num_sms, 1));
+    k_batch_reset<<<blocks, threads, 0, (cudaStream_t)stream>>>(d_status, d_steps, n, d_counts, n_counts, d_totals,
+                                                                 n_totals);
+    TB_CUDA(ctx, cudaGetLastError());
+    return TB_OK;
+}
+
 extern "C" int tb_step_monitors(tb_ctx *ctx, const tb_step_desc *d, const double *d_weights,
                                 const uint8_t *d_absolute, int n_monitors, double *d_out, void *stream) {
     if (!ctx || !d) return TB_ERR_ARG;

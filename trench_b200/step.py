@@ -486,10 +486,8 @@ class ChargingCase:
         L = _capi.lib()
         n = self.n_loaded if n is None else n
         s = self._stream()
-        self.status[:n].fill_(3)
-        self.steps[:n].zero_()
-        self.counts.zero_()
-        self.totals.zero_()
+        self.ctx.check(L.tb_batch_reset(self.ctx.handle, _ptr(self.status), _ptr(self.steps), n, _ptr(self.counts),
+                                        self.counts.numel(), _ptr(self.totals), self.totals.numel(), s))
         a = self._args
         precision = self._fill_args(n, buffer)
         ev = getattr(self, "trace_events", None)
@@ -502,9 +500,21 @@ class ChargingCase:
         if self.after_trace is not None:
             self.after_trace()
         self.ctx.check(L.tb_step_charge(self.ctx.handle, ctypes.byref(self._desc), s))
-        self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
+        # the charge monitors read only the new charge and the batch row: they run on a
+        # second stream beside the potential and field update (a fork and join inside a
+        # captured graph)
+        cur = torch.cuda.current_stream(self.dev)
+        if not hasattr(self, "_side"):
+            self._side = torch.cuda.Stream(self.dev)
+            self._ev_fork, self._ev_join = torch.cuda.Event(), torch.cuda.Event()
+        self._ev_fork.record(cur)
+        self._side.wait_event(self._ev_fork)
         self.ctx.check(L.tb_step_monitors(self.ctx.handle, ctypes.byref(self._desc), _ptr(self.t_mon_w),
-                                          _ptr(self.t_mon_abs), len(self.monitor_names), _ptr(self.qhist), s))
+                                          _ptr(self.t_mon_abs), len(self.monitor_names), _ptr(self.qhist),
+                                          ctypes.c_void_p(self._side.cuda_stream)))
+        self._ev_join.record(self._side)
+        self.ctx.check(L.tb_step_potential(self.ctx.handle, ctypes.byref(self._desc), s))
+        cur.wait_event(self._ev_join)
 
     TRACER_SHAPES = ((1024, 1), (768, 1), (512, 1), (512, 2), (256, 1), (128, 1))
 
