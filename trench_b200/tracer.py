@@ -14,6 +14,8 @@ in-flight clock; trajectory recording always uses the FP64 kernel.  There is no
 CPU path.
 """
 import ctypes
+import os
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 import torch
@@ -23,6 +25,56 @@ from .params import is_tapered
 
 CHUNK_STEPS = 256      # step budget per launch when a stop event must be polled
 DEFAULT_VSCALE = 1e5   # m/s, velocity unit of the FP32 state
+
+
+class _HostStager:
+    """Host-to-device copies of large pageable host arrays through two pinned staging
+    buffers: worker threads copy chunk k+1 into one buffer (NumPy copies release the
+    interpreter lock, so the host copy runs at several threads' bandwidth) while the copy
+    engine moves chunk k from the other, on a copy stream that the caller's stream then
+    waits for.  A plain pageable copy runs at one host thread's memcpy rate."""
+
+    CHUNK = 8 << 20
+
+    def __init__(self, device):
+        self.dev = device
+        self.pinned = [torch.empty(self.CHUNK, dtype=torch.uint8).pin_memory() for _ in range(2)]
+        self.host = [t.numpy() for t in self.pinned]
+        self.stream = torch.cuda.Stream(device)
+        self.events = [None, None]
+        self.k = 0
+        self.threads = max(1, min(8, os.cpu_count() or 1))
+        self.pool = ThreadPoolExecutor(self.threads) if self.threads > 1 else None
+
+    def _fill(self, dst, src):
+        n = src.size
+        if self.pool is None or n < (1 << 20):
+            np.copyto(dst, src)
+            return
+        step = -(-n // self.threads)
+        list(self.pool.map(lambda i: np.copyto(dst[i * step:(i + 1) * step], src[i * step:(i + 1) * step]),
+                           range(self.threads)))
+
+    def copy(self, dst, src):
+        """dst: contiguous 1-D device tensor; src: contiguous host array of dst's bytes."""
+        sb = src.reshape(-1).view(np.uint8)
+        db = dst.view(torch.uint8)
+        for off in range(0, sb.size, self.CHUNK):
+            j = self.k % 2
+            self.k += 1
+            ln = min(self.CHUNK, sb.size - off)
+            if self.events[j] is not None:
+                self.events[j].synchronize()        # the buffer's previous chunk has been copied
+            self._fill(self.host[j][:ln], sb[off:off + ln])
+            with torch.cuda.stream(self.stream):
+                db[off:off + ln].copy_(self.pinned[j][:ln], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.stream)
+            self.events[j] = ev
+
+    def join(self):
+        """The current stream waits for every copy issued so far."""
+        torch.cuda.current_stream(self.dev).wait_stream(self.stream)
 
 
 def _validate_rf(rf, n, shape):
@@ -96,6 +148,7 @@ class B200Tracer:
         self.precision = precision
         self.vscale = float(vscale)
         self.tdev = torch.device("cuda", self.device)
+        self._stager = None       # pinned staging of large host arrays (created on first use)
         self._last_dev = None     # device outputs of the last call, read back on first use of .last
         self._last_host = {}
         self._ctx_dx = None
@@ -138,8 +191,15 @@ class B200Tracer:
         view = self._buf(name, dtype, n)
         if isinstance(src, torch.Tensor):
             view.copy_(src.reshape(-1))
+            return view
+        host = np.ascontiguousarray(src, dtype=_np_dtype(dtype)).reshape(-1)
+        if host.nbytes >= (1 << 20):
+            if self._stager is None:
+                self._stager = _HostStager(self.tdev)
+            self._stager.copy(view, host)
+            self._stager.join()
         else:
-            view.copy_(torch.from_numpy(np.ascontiguousarray(src, dtype=_np_dtype(dtype)).reshape(-1)))
+            view.copy_(torch.from_numpy(host))
         return view
 
     def _fields(self, Ex, Ey, barrier):
