@@ -17,11 +17,14 @@ def small_sweep():
                     n_per_batch=1500 + 700 * i, n_batches=3) for i, p in enumerate(ps)]
 
 
-def test_pack_equals_cases_traced_one_by_one(cuda_device):
+@pytest.mark.parametrize("order", ["reverse", "learned", "index"])
+def test_pack_equals_cases_traced_one_by_one(cuda_device, order):
+    """Every claim order of the pack (the learned one through the batched ordering
+    kernels and claim records) gives each case's results bit for bit."""
     from trench_b200.batch import ChargingBatch
     from trench_b200.step import ChargingCase
     ps = small_sweep()
-    batch = ChargingBatch(ps, device=cuda_device, max_batches=4)
+    batch = ChargingBatch(ps, device=cuda_device, max_batches=4, claim_order=order)
     singles = [ChargingCase(p, device=cuda_device, precision="f32", max_batches=4) for p in ps]
     rngs = [np.random.default_rng(100 + i) for i in range(len(ps))]
     for _ in range(3):
@@ -40,12 +43,13 @@ def test_pack_equals_cases_traced_one_by_one(cuda_device):
             np.testing.assert_array_equal(hb[k], hc[k])
 
 
-def test_pack_graph_replay(cuda_device):
+@pytest.mark.parametrize("order", ["reverse", "learned"])
+def test_pack_graph_replay(cuda_device, order):
     import torch
     from trench_b200.batch import ChargingBatch
     ps = small_sweep()[:3]
-    a = ChargingBatch(ps, device=cuda_device, max_batches=4)
-    b = ChargingBatch(ps, device=cuda_device, max_batches=4)
+    a = ChargingBatch(ps, device=cuda_device, max_batches=4, claim_order=order)
+    b = ChargingBatch(ps, device=cuda_device, max_batches=4, claim_order=order)
     for i, p in enumerate(ps):
         parts = inject.inject(p, p.n_per_batch, a.cases[i].ny, np.random.default_rng(7 + i))
         a.load(i, *parts)

@@ -51,9 +51,10 @@ def sweep_params(n_cases, seed=0, base=None):
 class ChargingBatch:
     """circuits: optional list with one circuit per case (None for a case without
     circuit_rf), as ChargingCase takes; RF cases trace with their in-flight clock in the
-    same launch as the others."""
+    same launch as the others.  claim_order: one of CLAIM_ORDERS for every case's queue
+    (circuit_rf cases claim in index order under "learned")."""
 
-    def __init__(self, params, device=0, green="f64", max_batches=None, circuits=None):
+    def __init__(self, params, device=0, green="f64", max_batches=None, circuits=None, claim_order="learned"):
         if not params:
             raise ValueError("a batch needs at least one case")
         circuits = [None] * len(params) if circuits is None else list(circuits)
@@ -62,11 +63,14 @@ class ChargingBatch:
         self.dev = torch.device("cuda", int(device))
         self.cases = [ChargingCase(p, device=device, precision="f32", green=green, max_batches=max_batches,
                                    circuit=c) for p, c in zip(params, circuits)]
-        # each case's queue is claimed from its last particle down: a batch holds ions then
-        # electrons and the electrons run longest, so the pack's end is not left to them
-        # (64-case sweep: 13.7 -> 12.8 ms per batch)
+        # the pack ends with the particles claimed last in every case: the learned order
+        # (electrons first, then each case's ions longest predicted first, through the
+        # batched ordering kernels) leaves the short ones for the end (64-case sweep: 13.7 ms
+        # per batch in index order, 12.8 ms from the last particle down, 11.75 ms learned)
+        if claim_order not in CLAIM_ORDERS:
+            raise ValueError(f"claim_order must be one of {CLAIM_ORDERS}")
         for c in self.cases:
-            c.set_claim_order(CLAIM_ORDERS.index("reverse"))
+            c.set_claim_order(CLAIM_ORDERS.index(claim_order))
         L = _capi.lib()
         handles = (ctypes.c_void_p * len(self.cases))(*[c.ctx.handle.value for c in self.cases])
         h = ctypes.c_void_p()

@@ -53,8 +53,16 @@ struct K32 {
     int bytes;                      // packed field bytes (multiple of 16)
     int pool_off;                   // byte offset of the drain pool in dynamic shared memory, -1 = none
     int reverse;                    // claim particles from the last index down
-    const uint4 *rec;               // learned order: claim records in claim order (nullptr = none)
-    const unsigned *n_rec;          // learned order: number of records (device)
+    // learned claim order (nullptr rec = none): claim records in claim order, their number,
+    // each particle's key, the ion bins' classes, per-block class starts, per-bin step sums,
+    // 1 / domain width and the ordering kernels' blocks
+    uint4 *rec;
+    unsigned *n_rec;
+    uint16_t *okey;
+    uint8_t *oclass;
+    unsigned *oblk, *oacc;
+    double inv_lx;
+    int onb;
     // circuit_rf in flight (kernels with RF = true): the unit-voltage basis fields
     // (exs, eys, exm, eym) x vac in field units per padded cell, their per-face wall
     // barriers (substrate basis then mask basis, nx*ny each), the waveform per table
@@ -682,7 +690,9 @@ __global__ void __launch_bounds__(F32_THREADS, 1)
             int best = -1;
             for (int c = threadIdx.x; c < n_cases; c += 32) {
                 const unsigned long long q = *reinterpret_cast<volatile const unsigned long long *>(cases[c].queue);
-                const long long rem = cases[c].a.n - (long long)q;
+                // a case in the learned order queues only its traced particles (its records)
+                const long long lim = cases[c].rec ? (long long)*cases[c].n_rec : cases[c].a.n;
+                const long long rem = lim - (long long)q;
                 if (rem > best_rem) { best_rem = rem; best = c; }
             }
             for (int o = 16; o > 0; o >>= 1) {
@@ -710,6 +720,7 @@ __global__ void __launch_bounds__(F32_THREADS, 1)
         }
         uint32_t *pool = k.pool_off >= 0 ? reinterpret_cast<uint32_t *>(smem_raw + k.pool_off) : nullptr;
         if (k.a.n_phase > 0) run_case<SMEM, true>(k, fieldp, pool);  // block-uniform: one case per CTA
+        else if (SMEM && k.rec) run_case<SMEM, false, SMEM>(k, fieldp, pool);
         else run_case<SMEM, false>(k, fieldp, pool);
         __syncthreads();  // every warp is done with this case's field
     }
@@ -861,6 +872,11 @@ K32 make_k32(const tb_ctx *ctx, const tb_trace_args *a) {
     k.reverse = ctx->tune_reverse == 1;
     k.rec = nullptr;
     k.n_rec = nullptr;
+    k.okey = nullptr;
+    k.oclass = nullptr;
+    k.oblk = k.oacc = nullptr;
+    k.inv_lx = 0.0;
+    k.onb = 0;
     k.rf_field = ctx->d_rf_field;
     k.rf_barrier = ctx->d_rf_barrier;
     k.rf_wave = ctx->d_rf_wave;
@@ -907,6 +923,7 @@ __device__ __forceinline__ int claim_class(uint16_t key, const uint8_t *ion_clas
 // Blocks of the ordering kernels (k_claim_bins and k_claim_scatter walk the particles
 // with the same grid, so each block meets the same particles in both).
 constexpr int CLAIM_THREADS = 256;
+constexpr int PACK_CLAIM_BLOCKS = 64;   // ordering blocks per case of a pack
 int claim_blocks(const tb_ctx *ctx, long long n) {
     return (int)std::max<long long>(1, std::min<long long>((n + CLAIM_THREADS - 1) / CLAIM_THREADS,
                                                            4LL * std::max(ctx->num_sms, 1)));
@@ -914,13 +931,16 @@ int claim_blocks(const tb_ctx *ctx, long long n) {
 
 // Each particle's key (ion bin, electron, or not traced) and, per block, the number of
 // its particles in each class (blk[block][class]; warp-aggregated shared-memory counts).
-__global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k, double inv_lx, uint16_t *key,
-                                                              const uint8_t *ion_class, unsigned *blk) {
+// (block b of nb for the case of k)
+__device__ __forceinline__ void claim_bins_body(const K32 &k, int b, int nb) {
     __shared__ unsigned h[TB_ORDER_CLASSES];
     const tb_trace_args &a = k.a;
+    uint16_t *key = k.okey;
+    const uint8_t *ion_class = k.oclass;
+    const double inv_lx = k.inv_lx;
     if (threadIdx.x < TB_ORDER_CLASSES) h[threadIdx.x] = 0;
     __syncthreads();
-    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < a.n; i0 += (long long)gridDim.x * blockDim.x) {
+    for (long long i0 = (long long)b * blockDim.x; i0 < a.n; i0 += (long long)nb * blockDim.x) {
         const long long i = i0 + threadIdx.x;
         int c = TB_ORDER_CLASSES;
         if (i < a.n) {
@@ -937,7 +957,7 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k, doubl
         if (c < TB_ORDER_CLASSES && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[c], __popc(peers));
     }
     __syncthreads();
-    if (threadIdx.x < TB_ORDER_CLASSES) blk[blockIdx.x * TB_ORDER_CLASSES + threadIdx.x] = h[threadIdx.x];
+    if (threadIdx.x < TB_ORDER_CLASSES) k.oblk[b * TB_ORDER_CLASSES + threadIdx.x] = h[threadIdx.x];
 }
 
 // One block of 1024 threads (thread b for ordering block b, nb <= 1024): the start of
@@ -945,7 +965,7 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k, doubl
 // in turn within a class), written over the counts, and the number of records.  Each
 // thread scans its 16 counts within its warp; warp c then scans the warps' totals of
 // class c.
-__global__ void __launch_bounds__(1024) k_claim_scan(unsigned *blk, int nb, unsigned *n_rec) {
+__device__ __forceinline__ void claim_scan_body(unsigned *blk, int nb, unsigned *n_rec) {
     constexpr int C = TB_ORDER_CLASSES;
     __shared__ unsigned s_wsum[32][C + 1];   // per warp and class: the warp's total, then the warps before it
     __shared__ unsigned s_tot[C], s_start[C];
@@ -1018,15 +1038,16 @@ __global__ void __launch_bounds__(1024) k_claim_scan(unsigned *blk, int nb, unsi
 // state converted with the claim's expressions (cell, offset, velocity in vscale units,
 // q/m), the step count and species, and the particle index.  Places are handed out from
 // the block's starts with shared-memory counters.
-__global__ void __launch_bounds__(CLAIM_THREADS) k_claim_scatter(const K32 k, const uint16_t *key,
-                                                                 const uint8_t *ion_class, const unsigned *blk,
-                                                                 uint4 *rec) {
+__device__ __forceinline__ void claim_scatter_body(const K32 &k, int b, int nb) {
     __shared__ unsigned fill[TB_ORDER_CLASSES];
     const tb_trace_args &a = k.a;
+    const uint16_t *key = k.okey;
+    const uint8_t *ion_class = k.oclass;
+    uint4 *rec = k.rec;
     const int lane = threadIdx.x & 31;
-    if (threadIdx.x < TB_ORDER_CLASSES) fill[threadIdx.x] = blk[blockIdx.x * TB_ORDER_CLASSES + threadIdx.x];
+    if (threadIdx.x < TB_ORDER_CLASSES) fill[threadIdx.x] = k.oblk[b * TB_ORDER_CLASSES + threadIdx.x];
     __syncthreads();
-    for (long long i0 = (long long)blockIdx.x * blockDim.x; i0 < a.n; i0 += (long long)gridDim.x * blockDim.x) {
+    for (long long i0 = (long long)b * blockDim.x; i0 < a.n; i0 += (long long)nb * blockDim.x) {
         const long long i = i0 + threadIdx.x;
         int c = TB_ORDER_CLASSES;
         uint4 r0 = make_uint4(0u, 0u, 0u, 0u), r1 = r0;
@@ -1064,12 +1085,15 @@ __global__ void __launch_bounds__(CLAIM_THREADS) k_claim_scatter(const K32 k, co
 
 // After the trace: step sum and count of each ion bin (shared-memory histogram per block,
 // one global add per bin and block).
-__global__ void __launch_bounds__(1024) k_claim_learn(long long n, const uint16_t *key, const int32_t *steps,
-                                                      unsigned *acc) {
+__device__ __forceinline__ void claim_learn_body(const K32 &k, int blk_i, int nblk) {
     __shared__ unsigned h[2 * TB_ORDER_ION_BINS];
+    const long long n = k.a.n;
+    const uint16_t *key = k.okey;
+    const int32_t *steps = k.a.d_steps;
+    unsigned *acc = k.oacc;
     for (int b = threadIdx.x; b < 2 * TB_ORDER_ION_BINS; b += blockDim.x) h[b] = 0;
     __syncthreads();
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = (long long)blk_i * blockDim.x + threadIdx.x; i < n; i += (long long)nblk * blockDim.x) {
         const uint16_t kk = key[i];
         if (kk < TB_ORDER_ION_BINS) {
             atomicAdd(&h[2 * kk], (unsigned)steps[i]);
@@ -1084,7 +1108,7 @@ __global__ void __launch_bounds__(1024) k_claim_learn(long long n, const uint16_
 // Class of each ion bin for the next launch: 1 for the longest mean step count, then in
 // equal steps of that mean down to 15; bins without ions take the mean of all ions.  The
 // sums are cleared.
-__global__ void __launch_bounds__(TB_ORDER_ION_BINS) k_claim_classes(unsigned *acc, uint8_t *ion_class) {
+__device__ __forceinline__ void claim_classes_body(unsigned *acc, uint8_t *ion_class) {
     __shared__ float s_sum[TB_ORDER_ION_BINS], s_cnt[TB_ORDER_ION_BINS], s_max[TB_ORDER_ION_BINS];
     const int b = threadIdx.x;
     const float sum = (float)acc[2 * b], cnt = (float)acc[2 * b + 1];
@@ -1106,6 +1130,40 @@ __global__ void __launch_bounds__(TB_ORDER_ION_BINS) k_claim_classes(unsigned *a
     ion_class[b] = (uint8_t)min(max(c, 0), 14);
     acc[2 * b] = 0u;
     acc[2 * b + 1] = 0u;
+}
+
+// The ordering kernels of one case (grid = the case's ordering blocks) ...
+__global__ void __launch_bounds__(CLAIM_THREADS) k_claim_bins(const K32 k) { claim_bins_body(k, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(1024) k_claim_scan(const K32 k) { claim_scan_body(k.oblk, k.onb, k.n_rec); }
+__global__ void __launch_bounds__(CLAIM_THREADS) k_claim_scatter(const K32 k) {
+    claim_scatter_body(k, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(1024) k_claim_learn(const K32 k) { claim_learn_body(k, blockIdx.x, gridDim.x); }
+__global__ void __launch_bounds__(TB_ORDER_ION_BINS) k_claim_classes(const K32 k) {
+    claim_classes_body(k.oacc, k.oclass);
+}
+
+// ... and of every case of a pack that claims in the learned order (blockIdx.y or
+// blockIdx.x = case; cases without the order and surplus blocks return at once).
+__global__ void __launch_bounds__(CLAIM_THREADS) k_pack_claim_bins(const K32 *__restrict__ cases) {
+    const K32 &k = cases[blockIdx.y];
+    if (k.rec && (int)blockIdx.x < k.onb) claim_bins_body(k, blockIdx.x, k.onb);
+}
+__global__ void __launch_bounds__(1024) k_pack_claim_scan(const K32 *__restrict__ cases) {
+    const K32 &k = cases[blockIdx.x];
+    if (k.rec) claim_scan_body(k.oblk, k.onb, k.n_rec);
+}
+__global__ void __launch_bounds__(CLAIM_THREADS) k_pack_claim_scatter(const K32 *__restrict__ cases) {
+    const K32 &k = cases[blockIdx.y];
+    if (k.rec && (int)blockIdx.x < k.onb) claim_scatter_body(k, blockIdx.x, k.onb);
+}
+__global__ void __launch_bounds__(1024) k_pack_claim_learn(const K32 *__restrict__ cases) {
+    const K32 &k = cases[blockIdx.y];
+    if (k.rec) claim_learn_body(k, blockIdx.x, gridDim.x);
+}
+__global__ void __launch_bounds__(TB_ORDER_ION_BINS) k_pack_claim_classes(const K32 *__restrict__ cases) {
+    const K32 &k = cases[blockIdx.x];
+    if (k.rec) claim_classes_body(k.oacc, k.oclass);
 }
 
 // Learned-order buffers for n particles, allocated outside stream capture only; a failed
@@ -1156,6 +1214,19 @@ bool claim_buffers(tb_ctx *ctx, long long n, cudaStream_t s) {
     return true;
 }
 
+// The learned order's fields of a case's kernel arguments (its buffers must exist).
+void claim_fields(const tb_ctx *ctx, long long n, int nb, K32 *k) {
+    (void)n;
+    k->rec = ctx->d_claim_rec;
+    k->n_rec = ctx->d_claim_cls;
+    k->okey = ctx->d_claim_key;
+    k->oclass = ctx->d_ion_class;
+    k->oblk = ctx->d_claim_blk;
+    k->oacc = ctx->d_ion_acc;
+    k->inv_lx = 1.0 / (ctx->nx * ctx->dx);
+    k->onb = nb;
+}
+
 }  // namespace
 
 int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
@@ -1166,14 +1237,10 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     const bool learned = ctx->tune_reverse == 2 && !rf && a->n > 0 && a->n <= 0x7fffffffLL && ctx->nx < 65536 &&
                          ctx->ny < 32767 && 4 * ctx->num_sms <= 1024 && claim_buffers(ctx, a->n, s);
     if (learned) {
-        const double inv_lx = 1.0 / (ctx->nx * ctx->dx);
-        const int nb = claim_blocks(ctx, a->n);  // at most 4 x SMs <= 1024, one scan thread each
-        k_claim_bins<<<nb, CLAIM_THREADS, 0, s>>>(k, inv_lx, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_blk);
-        k_claim_scan<<<1, 1024, 0, s>>>(ctx->d_claim_blk, nb, ctx->d_claim_cls);
-        k_claim_scatter<<<nb, CLAIM_THREADS, 0, s>>>(k, ctx->d_claim_key, ctx->d_ion_class, ctx->d_claim_blk,
-                                                      ctx->d_claim_rec);
-        k.rec = ctx->d_claim_rec;
-        k.n_rec = ctx->d_claim_cls;
+        claim_fields(ctx, a->n, claim_blocks(ctx, a->n), &k);  // at most 4 x SMs <= 1024 blocks
+        k_claim_bins<<<k.onb, CLAIM_THREADS, 0, s>>>(k);
+        k_claim_scan<<<1, 1024, 0, s>>>(k);
+        k_claim_scatter<<<k.onb, CLAIM_THREADS, 0, s>>>(k);
     }
     const bool smem = k.bytes <= ctx->smem_attr_bytes;
     // CTA size and CTAs per SM come from the context's tuning (tb_set_tuning)
@@ -1219,8 +1286,8 @@ int tb_launch_trace_f32(tb_ctx *ctx, const tb_trace_args *a, cudaStream_t s) {
     else TB_LAUNCH_F32(1024);
 #undef TB_LAUNCH_F32
     if (learned) {
-        k_claim_learn<<<std::max(ctx->num_sms, 1), 1024, 0, s>>>(a->n, ctx->d_claim_key, a->d_steps, ctx->d_ion_acc);
-        k_claim_classes<<<1, TB_ORDER_ION_BINS, 0, s>>>(ctx->d_ion_acc, ctx->d_ion_class);
+        k_claim_learn<<<std::max(ctx->num_sms, 1), 1024, 0, s>>>(k);
+        k_claim_classes<<<1, TB_ORDER_ION_BINS, 0, s>>>(k);
     }
     TB_CUDA(ctx, cudaGetLastError());
     return TB_OK;
@@ -1338,6 +1405,7 @@ struct tb_pack {
     size_t launch_shm = 0;
     int num_sms = 0;
     int ready = 0;
+    int n_learned = 0;   // cases claimed in the learned order (tb_pack_set_args)
     tb_pack_steps *steps = nullptr;  // per-batch update of every case (tb_pack_set_steps)
     char err[512] = {0};
 };
@@ -1443,6 +1511,13 @@ extern "C" int tb_pack_set_args(tb_pack *p, const tb_trace_args *args) {
         ks[i] = make_k32(p->ctxs[i], &a);
         ks[i].queue = p->d_queues + i;
         ks[i].err = p->d_err;
+        // the learned claim order, for a case whose context asks for it and holds its buffers
+        // (tb_reserve_claim_order); its ordering kernels run over all such cases at once
+        // (shared-memory packs only: the global-memory pack kernel keeps its registers)
+        if (p->smem && c->tune_reverse == 2 && a.n_phase == 0 && a.n > 0 && c->nx < 65536 && c->ny < 32767 &&
+            c->d_claim_cls && a.n <= c->claim_cap)
+            claim_fields(c, a.n, (int)std::min<long long>((a.n + CLAIM_THREADS - 1) / CLAIM_THREADS, PACK_CLAIM_BLOCKS),
+                         &ks[i]);
         p->max_particles = std::max<int>(p->max_particles, (int)a.n);
     }
     // RF cases keep two more words per lane in the drain pool
@@ -1460,6 +1535,8 @@ extern "C" int tb_pack_set_args(tb_pack *p, const tb_trace_args *args) {
         }
     }
     for (int i = 0; i < p->n; ++i) ks[i].pool_off = p->launch_pool_off;
+    p->n_learned = 0;
+    for (int i = 0; i < p->n; ++i) p->n_learned += ks[i].rec != nullptr;
     cudaError_t e = cudaSetDevice(p->device);
     if (e == cudaSuccess) e = cudaMemcpy(p->d_cases, ks.data(), sizeof(K32) * p->n, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
@@ -1478,10 +1555,19 @@ extern "C" int tb_pack_trace(tb_pack *p, int reset, void *stream) {
         const int blocks = std::max(1, std::min(64, (p->max_particles + 255) / 256));
         k_pack_reset<<<dim3(blocks, p->n), 256, 0, s>>>(p->d_cases, p->n);
     }
+    if (p->n_learned) {  // claim records of the learned-order cases (after the reset)
+        k_pack_claim_bins<<<dim3(PACK_CLAIM_BLOCKS, p->n), CLAIM_THREADS, 0, s>>>(p->d_cases);
+        k_pack_claim_scan<<<p->n, 1024, 0, s>>>(p->d_cases);
+        k_pack_claim_scatter<<<dim3(PACK_CLAIM_BLOCKS, p->n), CLAIM_THREADS, 0, s>>>(p->d_cases);
+    }
     if (p->smem)
         trace_f32_batch_kernel<true><<<p->num_sms, F32_THREADS, p->launch_shm, s>>>(p->d_cases, p->n, p->d_err);
     else
         trace_f32_batch_kernel<false><<<p->num_sms, F32_THREADS, p->launch_shm, s>>>(p->d_cases, p->n, p->d_err);
+    if (p->n_learned) {
+        k_pack_claim_learn<<<dim3(PACK_CLAIM_BLOCKS / 4, p->n), 1024, 0, s>>>(p->d_cases);
+        k_pack_claim_classes<<<p->n, TB_ORDER_ION_BINS, 0, s>>>(p->d_cases);
+    }
     e = cudaGetLastError();
     if (e != cudaSuccess) return pack_fail(p, TB_ERR_CUDA, cudaGetErrorString(e));
     return TB_OK;
