@@ -518,8 +518,9 @@ def sweep_measure(steps, warmup, n_cases=64, cpu_seconds=15.0, accuracy=True):
                         "note": "36 B per particle-step + 28 B per particle over the case-pack tracer launch"},
            "l2": "flushed between timed steps (256 MiB write)", "clocks": clk,
            # per batch: the pack's reset and tracer launches, the charge update of all cases (one launch),
-           # the Green's products (one launch) and the fields (one launch)
-           "gpu_launches": 5 * steps,
+           # the Green's products (one launch) and the fields (one launch), and with the learned
+           # claim order its five batched ordering kernels
+           "gpu_launches": (5 + (5 if batch.cases[0].tuning.get("claim_order") == "learned" else 0)) * steps,
            "cpu_baseline": sweep_cpu_baseline(ps, seps, seconds_budget=cpu_seconds)}
     if accuracy:
         # the largest case of the pack, one batch from its charged state, FP32 vs FP64
