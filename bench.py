@@ -1057,6 +1057,7 @@ def steady_measure(p):
                         "(window 30, hold 2, at most 3000 batches)",
             "converged": bool(res["converged"]), "batches": nb, "seconds": wall, "batches_per_s": nb / wall,
             "particles_per_s": nb * 2 * q.n_per_batch / wall,
+            "tracer_shape": list(case.tuning.get("tracer_shape", ())), "claim_order": case.tuning.get("claim_order"),
             "steady_potentials_V": {k: round(v, 3) for k, v in res["steady"].items()}}
 
 
