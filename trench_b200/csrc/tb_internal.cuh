@@ -103,7 +103,7 @@ void tb_poisson_free(tb_poisson *ps);
 // starting column band and direction, each bin's mean step count is learned from the
 // previous trace, and the particles are claimed electrons first, then ions longest
 // predicted first, through a table of claim records written in that order.
-constexpr int TB_ORDER_ION_BINS = 256;   // 64 column bands x 4 direction bands
+constexpr int TB_ORDER_ION_BINS = 512;   // 128 column bands x 4 direction bands
 constexpr int TB_ORDER_CLASSES = 16;     // class 0 electrons, 1..15 ions by predicted length
 
 struct tb_ctx {

@@ -905,12 +905,12 @@ int pool_bytes(int threads, bool rf = false) { return (rf ? POOL_WORDS_RF : POOL
 // opening travel the whole trench (three to four times the steps of those stopped by the
 // mask), so they set the end.  The learned order claims every electron first (in index
 // order, as the reverse order does for a batch of ions then electrons) and then the ions
-// longest predicted first; the prediction is the mean step count of the ion's bin (64
+// longest predicted first; the prediction is the mean step count of the ion's bin (128
 // starting column bands x 4 bands of vx / |vy|) in the previous trace on this context.
 constexpr uint16_t KEY_NONE = 0xffff, KEY_ELECTRON = 0xfffe;
 
 __device__ __forceinline__ int ion_bin(double x, double vx, double vy, double inv_lx) {
-    const int xb = min(max((int)(x * inv_lx * 64.0), 0), 63);
+    const int xb = min(max((int)(x * inv_lx * 128.0), 0), 127);
     const double h = 0.1 * fabs(vy);
     const int db = vx < 0.0 ? (vx < -h ? 0 : 1) : (vx > h ? 3 : 2);
     return xb * 4 + db;
